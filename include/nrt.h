@@ -1,0 +1,207 @@
+/* nrt.h -- C ABI of the B200 NURBS ray-intersection engine (libnrt.so).
+ *
+ * The engine keeps the pipeline of Frostbite16/rt-nurbs as a drop-in:
+ *   knot-insertion Bezier decomposition  -> nrt_decompose / nrt_scene_create
+ *   SAH BVH over patch bounding boxes     -> nrt_build_bvh_binary / nrt_scene_create
+ *   per-ray traversal + rational Newton   -> nrt_intersect
+ *   pinhole primary rays                  -> nrt_generate_camera_rays
+ * Each entry point names the reference function it replaces (paths relative
+ * to the reference project root).
+ *
+ * Conventions
+ *  - Every function returns an nrt_status; on failure nrt_last_error() gives a
+ *    message (thread-local, valid until the next call on that thread).
+ *  - Device buffers are owned by the caller and passed as plain pointers.
+ *  - Device work is enqueued on the caller's stream (cudaStream_t passed as
+ *    void*, NULL = legacy default stream) and is asynchronous unless stated.
+ *  - A scene handle may be used from one stream at a time.
+ *  - Control points are weighted-homogeneous (w*x, w*y, w*z, w), float32,
+ *    exactly as ParametricSurf::nurbsSurf (src/math/nurbs.h:17-22).
+ */
+#ifndef NRT_H
+#define NRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NRT_OK = 0,
+    NRT_ERR_INVALID = 1,      /* bad argument (null pointer, size, degree) */
+    NRT_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    NRT_ERR_UNSUPPORTED = 3,  /* feature not available in this build / on this device */
+    NRT_ERR_DEVICE = 4,       /* a kernel reported an error (see nrt_last_error) */
+    NRT_ERR_NOMEM = 5         /* host or device allocation failed */
+} nrt_status;
+
+#define NRT_MAX_DEGREE 7
+
+/* One NURBS surface: ParametricSurf::nurbsSurf (src/math/nurbs.h:17-22).
+ * control_points: (n+1)*(m+1) points, index i*(m+1)+j, i along u.
+ * u_knots: n+p+2 values, v_knots: m+q+2 values (clamped). */
+typedef struct {
+    const float* control_points;
+    const float* u_knots;
+    const float* v_knots;
+    int n, m, p, q;
+} nrt_nurbs_surface;
+
+/* ------------------------------------------------------------------------
+ * Decomposition.  Replaces BezierPatchOps::getPatch (src/math/bezier_patch.h:86-139)
+ * with NurbsOps::decomposeSurface (src/math/nurbs.h:143-250), Algorithm A5.7,
+ * for degrees up to NRT_MAX_DEGREE (the reference caps at 4, src/constants.h:31-32).
+ * nrt_decompose_count gives nbU, nbV.  nrt_decompose writes nbU*nbV patches,
+ * patch (i,j) at i*nbV+j, each (p+1)*(q+1) points with index r*(q+1)+c, r
+ * along u, and ranges (u0,u1,v0,v1) per patch.  Host memory, synchronous.
+ * The arithmetic is float in the reference's order of operations, so the
+ * control points equal getPatch's bit for bit. */
+int nrt_decompose_count(const nrt_nurbs_surface* surf, int* nbU, int* nbV);
+int nrt_decompose(const nrt_nurbs_surface* surf, float* cp_out, float* ranges_out, int* nbU, int* nbV);
+
+/* Patch bounding boxes from the dehomogenised control points:
+ * BezierPatchOps::bounds (src/math/bezier_patch.h:153-169).  boxes: 6 floats
+ * per patch (min xyz, max xyz).  cp_offset[k] is the first point of patch k,
+ * degrees[2k..2k+1] = (p, q). Host, synchronous. */
+int nrt_patch_bounds(const float* cp, const int32_t* cp_offset, const int32_t* degrees, int n_patches, float* boxes);
+
+/* Binary BVH in the reference's node layout (BVHNode, src/core/bvh.h:13-17):
+ * node_bounds 6 floats, left_first, prim_count; inner nodes have prim_count 0
+ * and children left_first, left_first+1.  order[k] = input index of the
+ * primitive in leaf slot k (the reference reorders its patch array the same
+ * way, src/core/bvh.h:167-175).  Arrays hold 2N-1 nodes; *n_nodes gets the
+ * number used.  builder NRT_BVH_EXACT_SAH replaces BvhOps::buildBVH
+ * (src/core/bvh.h:148-179) node for node (O(N^2) per level, for small N);
+ * NRT_BVH_BINNED_SAH is the O(N log N) builder used for scenes. */
+enum { NRT_BVH_BINNED_SAH = 0, NRT_BVH_EXACT_SAH = 1 };
+int nrt_build_bvh_binary(const float* boxes, int n, int builder, float* node_bounds, uint32_t* left_first,
+                         uint32_t* prim_count, int32_t* order, int* n_nodes);
+
+/* ------------------------------------------------------------------------
+ * Scenes: decomposition + BVH + device upload in one call (the host pipeline
+ * of src/core/main.cpp:104-149 / src/core/benchmark.cpp:163-186).  The scene
+ * keeps its own device copy (patches packed SoA per patch, 16-byte aligned,
+ * in patch-local coordinates; a 4-wide BVH).  Patch ids reported by
+ * nrt_intersect are global patch indices in creation order: surface 0's
+ * patches first, each surface in getPatch order. */
+typedef struct nrt_scene nrt_scene;
+
+typedef struct {
+    int builder;        /* NRT_BVH_BINNED_SAH (default) or NRT_BVH_EXACT_SAH */
+    int max_leaf;       /* patches per BVH leaf (1..8, default 1) */
+    int device;         /* CUDA device ordinal */
+} nrt_build_opts;
+
+int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nrt_build_opts* opts,
+                     nrt_scene** out);
+/* Same from patches that are already decomposed (cp_offset/degrees as nrt_patch_bounds). */
+int nrt_scene_create_from_patches(const float* cp, const int32_t* cp_offset, const int32_t* degrees, int n_patches,
+                                  const nrt_build_opts* opts, nrt_scene** out);
+int nrt_scene_destroy(nrt_scene* scene);
+
+typedef struct {
+    int n_patches;
+    int n_surfaces;
+    int n_nodes;        /* 4-wide BVH nodes */
+    int bvh_depth;
+    size_t device_bytes;
+    int degree_hist[(NRT_MAX_DEGREE + 1) * (NRT_MAX_DEGREE + 1)]; /* patches per (p,q), index p*8+q */
+} nrt_scene_info;
+int nrt_scene_get_info(const nrt_scene* scene, nrt_scene_info* info);
+/* Global patch index -> (surface, patch within the surface, u0,u1,v0,v1). Host copies. */
+int nrt_scene_patch_table(const nrt_scene* scene, int32_t* surface_of, float* ranges);
+
+/* ------------------------------------------------------------------------
+ * Rays and hits: structure-of-arrays device buffers (SoAQueue::ray_queue,
+ * src/gpu/soa.h:6-14, without the idx_interact slot: misses are patch = -1). */
+typedef struct {
+    const float *ox, *oy, *oz;
+    const float *dx, *dy, *dz;
+} nrt_rays;
+
+typedef struct {
+    float *ox, *oy, *oz;
+    float *dx, *dy, *dz;
+} nrt_rays_out;
+
+/* Hit record per ray.  patch = -1 on a miss.  t is the distance along the ray
+ * in units of |d| (the reference's t, src/gpu/intersect.cu:129-131, which
+ * assumes |d| = 1), (u, v) are patch-local in [0,1].  Optional arrays may be
+ * NULL: iters (Newton evaluations of the accepted solve), tests (patch tests
+ * that ran Newton), geom (9 floats: S, dS/du, dS/dv in world space, as
+ * surfaceInteraction's dpdu/dpdv, src/gpu/interact.h:6-21). */
+typedef struct {
+    int32_t* patch;
+    float* t;
+    float* u;
+    float* v;
+    int32_t* iters;
+    int32_t* tests;
+    float* geom;
+} nrt_hits;
+
+enum { NRT_INIT_MIDPOINT = 0, NRT_INIT_BILINEAR = 1, NRT_INIT_LEARNED = 2 };
+enum { NRT_SCHED_PIXEL = 0, NRT_SCHED_WAVEFRONT = 1 };
+
+typedef struct {
+    int init_mode;        /* NRT_INIT_*: (0.5,0.5); the reference's bilinear guess
+                             (src/math/bezier_patch.h:272-327); or the learned MLP */
+    int max_iter;         /* Newton evaluations per (ray, patch); the reference uses 7 */
+    float eps;            /* converged when |r1|+|r2| < eps; the reference uses 1e-4 */
+    float det_eps;        /* |det J| below this takes the seeded pull step (1e-5) */
+    float cond_fp64;      /* solve the 2x2 step in FP64 when cond(J) exceeds this; 0 = never */
+    int fp64_final;       /* 1: one FP64 Newton step on the converged point */
+    int hull_cull;        /* 1: skip (ray, patch) tests whose control points all lie on
+                             one side of a ray plane by more than eps (result unchanged) */
+    int schedule;         /* NRT_SCHED_PIXEL or NRT_SCHED_WAVEFRONT */
+    int seed_offset;      /* added to the ray index to seed the singular-Jacobian pull */
+    float flat_threshold; /* flat-skip in pixels (src/gpu/intersect.cu:104-123); 0 = off */
+    float cam_k;          /* 0.5*H/tan(vfov/2), only used by flat-skip */
+} nrt_intersect_opts;
+
+/* Fill opts with the plain settings: midpoint init, 8 evaluations, eps 1e-6,
+ * det_eps 1e-5, no FP64, no cull, per-pixel schedule. */
+void nrt_default_opts(nrt_intersect_opts* opts);
+/* The reference's settings (calculateIntersectWrapper, src/gpu/intersect.cu:199-220):
+ * bilinear init, 7 evaluations, eps 1e-4, det_eps 1e-5. */
+void nrt_reference_opts(nrt_intersect_opts* opts);
+
+/* Closest hit for n rays.  Replaces calculateIntersectWrapper /
+ * calculateIntersect (src/gpu/intersect.h:9-13, src/gpu/intersect.cu:20-220).
+ * Asynchronous on `stream`; device buffers; n may be 0. */
+int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                  const nrt_hits* hits, void* stream);
+
+/* Counters of the last nrt_intersect on this scene (synchronises the stream). */
+typedef struct {
+    uint64_t rays, box_tests, patch_candidates, patch_culled, newton_solves, newton_evals, fp64_solves,
+        fp64_final_steps, hits, errors;
+    uint64_t evals_by_degree[64];      /* Newton evaluations per (p,q), index p*8+q */
+    uint64_t hull_tests_by_degree[64]; /* hull tests per (p,q) */
+} nrt_counters;
+int nrt_enable_counters(nrt_scene* scene, int enable);
+int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Pinhole camera rays.  Replaces calculateRaysWrapper / calculateRays<perspective>
+ * (src/gpu/generateRaysKernel.cu:15-69, src/core/camera.h:63-174): eye, look,
+ * up as Transform::lookAt; vertical (short-axis) field of view in degrees;
+ * ray index (y*W + x)*spp + s; spp = 1 uses the pixel centre, spp > 1 jitters
+ * with a seeded PCG hash.  Directions are unit length. */
+typedef struct {
+    float eye[3], look[3], up[3];
+    float fov_deg;
+    int width, height, spp;
+    uint32_t seed;
+} nrt_camera;
+int nrt_generate_camera_rays(const nrt_camera* cam, const nrt_rays_out* out, void* stream);
+
+const char* nrt_last_error(void);
+const char* nrt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NRT_H */

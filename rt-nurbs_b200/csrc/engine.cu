@@ -1,0 +1,514 @@
+// engine.cu -- the C ABI (include/nrt.h): host pipeline, device packing,
+// launches and error reporting.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "nrt_internal.h"
+
+// ---------------------------------------------------------------------------
+namespace nrt {
+
+static thread_local std::string g_error;
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+}
+
+int fail(int status, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return status;
+}
+
+static int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? NRT_ERR_NOMEM : NRT_ERR_CUDA, "%s: %s (%s)", what,
+                cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define NRT_CUDA(call, what)                               \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// Flatness of a patch: largest distance from a control point to the bilinear
+// interpolation of the four corners at its (i/p, j/q) node; patchDelta,
+// src/core/main.cpp:18-43.
+static float patch_delta(const float* P, int p, int q) {
+    const int row = q + 1;
+    auto dh = [&](int i, float o[3]) {
+        const float iw = 1.0f / P[4 * i + 3];
+        o[0] = P[4 * i] * iw; o[1] = P[4 * i + 1] * iw; o[2] = P[4 * i + 2] * iw;
+    };
+    float c00[3], c10[3], c01[3], c11[3];
+    dh(0, c00); dh(p * row, c10); dh(q, c01); dh(p * row + q, c11);
+    float d = 0.f;
+    for (int i = 0; i <= p; ++i)
+        for (int j = 0; j <= q; ++j) {
+            const float u = (float)i / p, v = (float)j / q;
+            const float a = (1 - u) * (1 - v), b = u * (1 - v), c = (1 - u) * v, e = u * v;
+            float Pij[3];
+            dh(i * row + j, Pij);
+            float s = 0.f;
+            for (int k = 0; k < 3; ++k) {
+                const float B = a * c00[k] + b * c10[k] + c * c01[k] + e * c11[k];
+                s += (Pij[k] - B) * (Pij[k] - B);
+            }
+            d = fmaxf(d, sqrtf(s));
+        }
+    return d;
+}
+
+}  // namespace nrt
+
+using namespace nrt;
+
+struct nrt_scene {
+    int device = 0;
+    PatchSet ps;
+    int n_surfaces = 0;
+    std::vector<int32_t> slot_patch;   // device slot -> global patch id
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    unsigned long long* counters = nullptr;
+    int counters_on = 0;
+    dev::Scene view{};
+    nrt_scene_info info{};
+};
+
+namespace {
+
+int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_scene** out) {
+    if (!out) return fail(NRT_ERR_INVALID, "out is null");
+    *out = nullptr;
+    const int N = ps.count();
+    if (N <= 0) return fail(NRT_ERR_INVALID, "scene has no patches");
+    nrt_build_opts o{NRT_BVH_BINNED_SAH, 1, 0};
+    if (opts) o = *opts;
+    if (o.max_leaf < 1 || o.max_leaf > 8) return fail(NRT_ERR_INVALID, "max_leaf must be in 1..8");
+    if (N >= (1 << 27)) return fail(NRT_ERR_INVALID, "too many patches (%d)", N);
+    for (int k = 0; k < N; ++k) {
+        const int p = ps.deg[2 * k], q = ps.deg[2 * k + 1];
+        if (p < 1 || q < 1 || p > NRT_MAX_DEGREE || q > NRT_MAX_DEGREE)
+            return fail(NRT_ERR_INVALID, "patch %d has degree (%d,%d) outside 1..%d", k, p, q, NRT_MAX_DEGREE);
+    }
+    // BVH over patch boxes
+    std::vector<Box3> boxes;
+    patch_boxes(ps, boxes);
+    BinaryBVH bin;
+    if (o.builder == NRT_BVH_EXACT_SAH) build_exact_sah(boxes, bin);
+    else build_binned_sah(boxes, o.max_leaf, bin);
+    for (int i = 0; i < bin.used; ++i)
+        if (bin.prim_count[i] > 8)  // coincident centroids can leave bigger leaves
+            return fail(NRT_ERR_UNSUPPORTED, "BVH leaf with %u patches (limit 8)", bin.prim_count[i]);
+    std::vector<Node4> wide;
+    int depth = 0;
+    collapse_to_wide(bin, wide, depth);
+
+    // Pack patches in leaf order.
+    std::vector<int4> hdr(N);
+    std::vector<double4> centre(N);
+    std::vector<float4> corners(4 * (size_t)N);
+    std::vector<float> delta(N);
+    std::vector<float> blocks;
+    std::vector<int32_t> slot_patch(N);
+    size_t total_floats = 0;
+    for (int s = 0; s < N; ++s) {
+        const int k = bin.order[s];
+        total_floats += 4 * (size_t)dev::padded_points(ps.deg[2 * k], ps.deg[2 * k + 1]);
+    }
+    blocks.assign(total_floats, 0.f);
+    size_t off = 0;
+    nrt_scene_info info{};
+    for (int s = 0; s < N; ++s) {
+        const int k = bin.order[s];
+        slot_patch[s] = k;
+        const int p = ps.deg[2 * k], q = ps.deg[2 * k + 1], n = (p + 1) * (q + 1);
+        const int np = dev::padded_points(p, q);
+        const float* P = &ps.cp[4 * (size_t)ps.off[k]];
+        const Box3& b = boxes[k];
+        const double cx = 0.5 * ((double)b.lo[0] + b.hi[0]), cy = 0.5 * ((double)b.lo[1] + b.hi[1]),
+                     cz = 0.5 * ((double)b.lo[2] + b.hi[2]);
+        bool pos = true;
+        double rad = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double w = P[4 * i + 3];
+            pos = pos && (w > 0.0);
+            blocks[off + i] = (float)((double)P[4 * i + 0] - w * cx);
+            blocks[off + np + i] = (float)((double)P[4 * i + 1] - w * cy);
+            blocks[off + 2 * np + i] = (float)((double)P[4 * i + 2] - w * cz);
+            blocks[off + 3 * np + i] = (float)w;
+            if (w != 0.0) {
+                const double dx = P[4 * i] / w - cx, dy = P[4 * i + 1] / w - cy, dz = P[4 * i + 2] / w - cz;
+                rad = std::max(rad, std::sqrt(dx * dx + dy * dy + dz * dz));
+            }
+        }
+        for (int i = n; i < np; ++i) blocks[off + 3 * np + i] = 1.f;  // padding never read as a point
+        hdr[s] = make_int4((int)off, p | (q << 4) | ((pos ? dev::kFlagPositiveWeights : 0) << 8), k, ps.surf[k]);
+        centre[s] = make_double4(cx, cy, cz, rad);
+        const int ci[4] = {0, p * (q + 1), p * (q + 1) + q, q};  // q00, q10, q11, q01 (bezier_patch.h:37-44)
+        for (int c = 0; c < 4; ++c) {
+            const float* X = P + 4 * ci[c];
+            const float iw = 1.f / X[3];
+            corners[4 * (size_t)s + c] = make_float4(X[0] * iw, X[1] * iw, X[2] * iw, 0.f);
+        }
+        delta[s] = patch_delta(P, p, q);
+        info.degree_hist[p * 8 + q] += 1;
+        off += 4 * (size_t)np;
+    }
+
+    // One device arena, every array 256-byte aligned.
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t sz_nodes = align(wide.size() * sizeof(Node4)), sz_hdr = align(N * sizeof(int4)),
+                 sz_cen = align(N * sizeof(double4)), sz_cp = align(blocks.size() * sizeof(float)),
+                 sz_cor = align(corners.size() * sizeof(float4)), sz_del = align(N * sizeof(float)),
+                 sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long));
+    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr;
+    nrt_scene* sc = new (std::nothrow) nrt_scene();
+    if (!sc) return fail(NRT_ERR_NOMEM, "host allocation failed");
+    sc->device = o.device;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaError_t e = cudaSetDevice(o.device);
+    if (e != cudaSuccess) { delete sc; return cuda_fail(e, "cudaSetDevice"); }
+    e = cudaMalloc(&sc->arena, total);
+    if (e != cudaSuccess) { delete sc; cudaSetDevice(prev); return cuda_fail(e, "cudaMalloc(scene)"); }
+    char* base = static_cast<char*>(sc->arena);
+    size_t at = 0;
+    auto put = [&](const void* src, size_t bytes, size_t slot) -> void* {
+        void* dst = base + at;
+        if (bytes) e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+        at += slot;
+        return dst;
+    };
+    sc->view.nodes = static_cast<const dev::Node4*>(put(wide.data(), wide.size() * sizeof(Node4), sz_nodes));
+    sc->view.hdr = static_cast<const int4*>(put(hdr.data(), N * sizeof(int4), sz_hdr));
+    sc->view.centre = static_cast<const double4*>(put(centre.data(), N * sizeof(double4), sz_cen));
+    sc->view.cp = static_cast<const float*>(put(blocks.data(), blocks.size() * sizeof(float), sz_cp));
+    sc->view.corners = static_cast<const float4*>(put(corners.data(), corners.size() * sizeof(float4), sz_cor));
+    sc->view.delta = static_cast<const float*>(put(delta.data(), N * sizeof(float), sz_del));
+    sc->counters = reinterpret_cast<unsigned long long*>(base + at);
+    if (e == cudaSuccess) e = cudaMemset(sc->counters, 0, sz_ctr);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaFree(sc->arena);
+        delete sc;
+        return cuda_fail(e, "scene upload");
+    }
+    sc->view.n_slots = N;
+    sc->arena_bytes = total;
+    info.n_patches = N;
+    info.n_surfaces = n_surfaces;
+    info.n_nodes = (int)wide.size();
+    info.bvh_depth = depth;
+    info.device_bytes = total;
+    sc->info = info;
+    sc->slot_patch = std::move(slot_patch);
+    sc->ps = std::move(ps);
+    sc->n_surfaces = n_surfaces;
+    *out = sc;
+    return NRT_OK;
+}
+
+void to_dev_opts(const nrt_intersect_opts& o, dev::Opts& d, int counters) {
+    d.nw.max_iter = o.max_iter;
+    d.nw.eps = o.eps;
+    d.nw.det_eps = o.det_eps;
+    d.nw.cond_fp64 = o.cond_fp64;
+    d.nw.fp64_final = o.fp64_final;
+    d.init_mode = o.init_mode;
+    d.hull_cull = o.hull_cull;
+    d.seed_offset = (uint32_t)o.seed_offset;
+    d.flat_threshold = o.flat_threshold;
+    d.cam_k = o.cam_k;
+    d.counters = counters;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* nrt_last_error(void) { return g_error.c_str(); }
+const char* nrt_version(void) { return "nrt 0.1 (sm_100a)"; }
+
+int nrt_decompose_count(const nrt_nurbs_surface* surf, int* nbU, int* nbV) {
+    if (!surf || !nbU || !nbV) return fail(NRT_ERR_INVALID, "null argument");
+    if (int st = check_surface(*surf)) return st;
+    int nu = 1, nv = 1;
+    for (int i = surf->p + 1; i <= surf->n; ++i) nu += surf->u_knots[i] != surf->u_knots[i - 1];
+    for (int j = surf->q + 1; j <= surf->m; ++j) nv += surf->v_knots[j] != surf->v_knots[j - 1];
+    *nbU = nu;
+    *nbV = nv;
+    return NRT_OK;
+}
+
+int nrt_decompose(const nrt_nurbs_surface* surf, float* cp_out, float* ranges_out, int* nbU, int* nbV) {
+    if (!surf || !cp_out || !nbU || !nbV) return fail(NRT_ERR_INVALID, "null argument");
+    std::vector<float> cp, ranges;
+    int nu = 0, nv = 0;
+    if (int st = decompose_surface(*surf, cp, ranges, nu, nv)) return st;
+    std::memcpy(cp_out, cp.data(), cp.size() * sizeof(float));
+    if (ranges_out) std::memcpy(ranges_out, ranges.data(), ranges.size() * sizeof(float));
+    *nbU = nu;
+    *nbV = nv;
+    return NRT_OK;
+}
+
+int nrt_patch_bounds(const float* cp, const int32_t* cp_offset, const int32_t* degrees, int n_patches,
+                     float* boxes) {
+    if (n_patches < 0 || (n_patches > 0 && (!cp || !cp_offset || !degrees || !boxes)))
+        return fail(NRT_ERR_INVALID, "null argument");
+    PatchSet ps;
+    int max_point = 0;
+    for (int k = 0; k < n_patches; ++k)
+        max_point = std::max(max_point, cp_offset[k] + (degrees[2 * k] + 1) * (degrees[2 * k + 1] + 1));
+    ps.cp.assign(cp, cp + 4 * (size_t)max_point);
+    ps.off.assign(cp_offset, cp_offset + n_patches);
+    ps.deg.assign(degrees, degrees + 2 * (size_t)n_patches);
+    std::vector<Box3> b;
+    patch_boxes(ps, b);
+    for (int k = 0; k < n_patches; ++k)
+        for (int a = 0; a < 3; ++a) { boxes[6 * k + a] = b[k].lo[a]; boxes[6 * k + 3 + a] = b[k].hi[a]; }
+    return NRT_OK;
+}
+
+int nrt_build_bvh_binary(const float* boxes, int n, int builder, float* node_bounds, uint32_t* left_first,
+                         uint32_t* prim_count, int32_t* order, int* n_nodes) {
+    if (n <= 0 || !boxes || !node_bounds || !left_first || !prim_count || !order)
+        return fail(NRT_ERR_INVALID, "null argument or empty input");
+    std::vector<Box3> prims(n);
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) { prims[i].lo[a] = boxes[6 * i + a]; prims[i].hi[a] = boxes[6 * i + 3 + a]; }
+    BinaryBVH bin;
+    if (builder == NRT_BVH_EXACT_SAH) build_exact_sah(prims, bin);
+    else if (builder == NRT_BVH_BINNED_SAH) build_binned_sah(prims, 1, bin);
+    else return fail(NRT_ERR_INVALID, "unknown BVH builder %d", builder);
+    const size_t M = 2 * (size_t)n - 1;
+    for (size_t i = 0; i < M; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            node_bounds[6 * i + a] = bin.box[i].lo[a];
+            node_bounds[6 * i + 3 + a] = bin.box[i].hi[a];
+        }
+        left_first[i] = bin.left_first[i];
+        prim_count[i] = bin.prim_count[i];
+    }
+    std::memcpy(order, bin.order.data(), sizeof(int32_t) * n);
+    if (n_nodes) *n_nodes = bin.used;
+    return NRT_OK;
+}
+
+int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nrt_build_opts* opts,
+                     nrt_scene** out) {
+    if (!surfaces || n_surfaces <= 0 || !out) return fail(NRT_ERR_INVALID, "null or empty surface list");
+    PatchSet ps;
+    for (int si = 0; si < n_surfaces; ++si) {
+        std::vector<float> cp, ranges;
+        int nu = 0, nv = 0;
+        if (int st = decompose_surface(surfaces[si], cp, ranges, nu, nv)) {
+            set_error("surface %d: %s", si, nrt_last_error());
+            return st;
+        }
+        const int piece = (surfaces[si].p + 1) * (surfaces[si].q + 1);
+        const int base = (int)(ps.cp.size() / 4);
+        ps.cp.insert(ps.cp.end(), cp.begin(), cp.end());
+        ps.ranges.insert(ps.ranges.end(), ranges.begin(), ranges.end());
+        for (int k = 0; k < nu * nv; ++k) {
+            ps.off.push_back(base + k * piece);
+            ps.deg.push_back(surfaces[si].p);
+            ps.deg.push_back(surfaces[si].q);
+            ps.surf.push_back(si);
+        }
+    }
+    return build_scene(std::move(ps), n_surfaces, opts, out);
+}
+
+int nrt_scene_create_from_patches(const float* cp, const int32_t* cp_offset, const int32_t* degrees, int n_patches,
+                                  const nrt_build_opts* opts, nrt_scene** out) {
+    if (!cp || !cp_offset || !degrees || n_patches <= 0 || !out) return fail(NRT_ERR_INVALID, "null or empty input");
+    PatchSet ps;
+    int max_point = 0;
+    for (int k = 0; k < n_patches; ++k) {
+        if (cp_offset[k] < 0) return fail(NRT_ERR_INVALID, "negative control point offset");
+        max_point = std::max(max_point, cp_offset[k] + (degrees[2 * k] + 1) * (degrees[2 * k + 1] + 1));
+    }
+    ps.cp.assign(cp, cp + 4 * (size_t)max_point);
+    ps.off.assign(cp_offset, cp_offset + n_patches);
+    ps.deg.assign(degrees, degrees + 2 * (size_t)n_patches);
+    ps.ranges.assign(4 * (size_t)n_patches, 0.f);
+    for (int k = 0; k < n_patches; ++k) { ps.ranges[4 * k + 1] = 1.f; ps.ranges[4 * k + 3] = 1.f; }
+    ps.surf.assign(n_patches, 0);
+    return build_scene(std::move(ps), 1, opts, out);
+}
+
+int nrt_scene_destroy(nrt_scene* scene) {
+    if (!scene) return NRT_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    cudaError_t e = cudaFree(scene->arena);
+    cudaSetDevice(prev);
+    delete scene;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFree(scene)");
+    return NRT_OK;
+}
+
+int nrt_scene_get_info(const nrt_scene* scene, nrt_scene_info* info) {
+    if (!scene || !info) return fail(NRT_ERR_INVALID, "null argument");
+    *info = scene->info;
+    return NRT_OK;
+}
+
+int nrt_scene_patch_table(const nrt_scene* scene, int32_t* surface_of, float* ranges) {
+    if (!scene) return fail(NRT_ERR_INVALID, "null scene");
+    const int N = scene->ps.count();
+    if (surface_of) std::memcpy(surface_of, scene->ps.surf.data(), sizeof(int32_t) * N);
+    if (ranges) std::memcpy(ranges, scene->ps.ranges.data(), sizeof(float) * 4 * N);
+    return NRT_OK;
+}
+
+void nrt_default_opts(nrt_intersect_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->init_mode = NRT_INIT_MIDPOINT;
+    o->max_iter = 8;
+    o->eps = 1e-6f;
+    o->det_eps = 1e-5f;
+    o->cond_fp64 = 0.f;
+    o->fp64_final = 0;
+    o->hull_cull = 0;
+    o->schedule = NRT_SCHED_PIXEL;
+}
+
+void nrt_reference_opts(nrt_intersect_opts* o) {
+    nrt_default_opts(o);
+    if (!o) return;
+    o->init_mode = NRT_INIT_BILINEAR;
+    o->max_iter = 7;
+    o->eps = 1e-4f;
+}
+
+int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                  const nrt_hits* hits, void* stream) {
+    if (!scene || !rays || !opts || !hits) return fail(NRT_ERR_INVALID, "null argument");
+    if (n < 0) return fail(NRT_ERR_INVALID, "negative ray count");
+    if (n == 0) return NRT_OK;
+    if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz)
+        return fail(NRT_ERR_INVALID, "null ray array");
+    if (!hits->patch || !hits->t || !hits->u || !hits->v) return fail(NRT_ERR_INVALID, "null hit array");
+    const nrt_intersect_opts& o = *opts;
+    if (o.max_iter < 1 || o.max_iter > 256) return fail(NRT_ERR_INVALID, "max_iter %d outside 1..256", o.max_iter);
+    if (!(o.eps > 0.f)) return fail(NRT_ERR_INVALID, "eps must be positive");
+    if (o.init_mode != NRT_INIT_MIDPOINT && o.init_mode != NRT_INIT_BILINEAR) {
+        if (o.init_mode == NRT_INIT_LEARNED) return fail(NRT_ERR_UNSUPPORTED, "learned init needs a trained model");
+        return fail(NRT_ERR_INVALID, "unknown init mode %d", o.init_mode);
+    }
+    if (o.schedule != NRT_SCHED_PIXEL) return fail(NRT_ERR_UNSUPPORTED, "schedule %d not available", o.schedule);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != scene->device) NRT_CUDA(cudaSetDevice(scene->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    dev::Opts d;
+    to_dev_opts(o, d, scene->counters_on);
+    if (scene->counters_on)
+        NRT_CUDA(cudaMemsetAsync(scene->counters, 0, dev::kCounterWords * sizeof(unsigned long long), st),
+                 "counter reset");
+    dev::Rays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz};
+    dev::Hits h{hits->patch, hits->t, hits->u, hits->v, hits->iters, hits->tests, hits->geom};
+    cudaError_t e = dev::launch_intersect_pixel(scene->view, r, (long long)n, d, h, scene->counters, st);
+    if (prev != scene->device) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
+    return NRT_OK;
+}
+
+int nrt_enable_counters(nrt_scene* scene, int enable) {
+    if (!scene) return fail(NRT_ERR_INVALID, "null scene");
+    scene->counters_on = enable ? 1 : 0;
+    return NRT_OK;
+}
+
+int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
+    if (!scene || !out) return fail(NRT_ERR_INVALID, "null argument");
+    unsigned long long h[dev::kCounterWords];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NRT_CUDA(cudaMemcpyAsync(h, scene->counters, sizeof(h), cudaMemcpyDeviceToHost, st), "counter read");
+    NRT_CUDA(cudaStreamSynchronize(st), "counter sync");
+    out->rays = h[dev::kRays];
+    out->box_tests = h[dev::kBoxTests];
+    out->patch_candidates = h[dev::kCandidates];
+    out->patch_culled = h[dev::kCulled];
+    out->newton_solves = h[dev::kSolves];
+    out->newton_evals = h[dev::kEvals];
+    out->fp64_solves = h[dev::kFp64Solves];
+    out->fp64_final_steps = h[dev::kFp64Final];
+    out->hits = h[dev::kHits];
+    out->errors = h[dev::kErrors];
+    for (int k = 0; k < 64; ++k) {
+        out->evals_by_degree[k] = h[dev::kEvalsByDegree + k];
+        out->hull_tests_by_degree[k] = h[dev::kHullByDegree + k];
+    }
+    if (out->errors) return fail(NRT_ERR_DEVICE, "kernel reported %llu errors (traversal stack or degree)",
+                                 (unsigned long long)out->errors);
+    return NRT_OK;
+}
+
+int nrt_generate_camera_rays(const nrt_camera* cam, const nrt_rays_out* out, void* stream) {
+    if (!cam || !out || !out->ox || !out->oy || !out->oz || !out->dx || !out->dy || !out->dz)
+        return fail(NRT_ERR_INVALID, "null argument");
+    if (cam->width <= 0 || cam->height <= 0 || cam->spp <= 0) return fail(NRT_ERR_INVALID, "empty image");
+    if (!(cam->fov_deg > 0.f && cam->fov_deg < 180.f)) return fail(NRT_ERR_INVALID, "fov outside (0,180)");
+    // camera basis in double, unfused, as Transform::lookAt (src/math/transform.h:46-60)
+    auto norm = [](double v[3]) {
+        const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double il = 1.0 / l;
+        v[0] = v[0] * il; v[1] = v[1] * il; v[2] = v[2] * il;
+    };
+    auto cross = [](const double a[3], const double b[3], double o[3]) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    dev::CameraParams cp{};
+    double E[3] = {cam->eye[0], cam->eye[1], cam->eye[2]}, L[3] = {cam->look[0], cam->look[1], cam->look[2]},
+           U[3] = {cam->up[0], cam->up[1], cam->up[2]};
+    double f[3] = {L[0] - E[0], L[1] - E[1], L[2] - E[2]};
+    norm(f);
+    double rt[3];
+    cross(U, f, rt);
+    norm(rt);
+    double up[3];
+    cross(f, rt, up);
+    for (int a = 0; a < 3; ++a) { cp.eye[a] = E[a]; cp.fwd[a] = f[a]; cp.right[a] = rt[a]; cp.up[a] = up[a]; }
+    const double aspect = (double)cam->width / (double)cam->height;
+    if (aspect > 1.0) { cp.x0 = -aspect; cp.x1 = aspect; cp.y0 = -1; cp.y1 = 1; }
+    else { cp.x0 = -1; cp.x1 = 1; cp.y0 = -1.0 / aspect; cp.y1 = 1.0 / aspect; }
+    cp.tan_half = std::tan((double)cam->fov_deg * (3.14159265358979323846 / 180.0) / 2.0);
+    cp.width = cam->width;
+    cp.height = cam->height;
+    cp.spp = cam->spp;
+    cp.seed = cam->seed;
+    cudaError_t e = dev::launch_camera_rays(cp, out->ox, out->oy, out->oz, out->dx, out->dy, out->dz,
+                                            static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "camera ray launch");
+    return NRT_OK;
+}
+
+}  // extern "C"

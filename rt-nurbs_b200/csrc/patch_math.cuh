@@ -1,0 +1,419 @@
+// patch_math.cuh -- per-(ray, patch) device math of the intersection path.
+//
+// Patches live on the device in patch-local coordinates: every patch has a
+// centre C (double) and its control points are stored as
+// (w*(x-Cx), w*(y-Cy), w*(z-Cz), w) in FP32, one SoA block per patch
+// (X[np] Y[np] Z[np] W[np], np = (p+1)(q+1) rounded up to 4, 16-byte aligned).
+// The ray's two planes n_k.x + d_k = 0 (MathUtils::getRayPlanes,
+// src/math/math_utils.h:33-54) become n_k.S_loc + e_k with e_k = -n_k.(O - C)
+// computed in FP64 once per (ray, patch); |e_k| is the distance from the ray to
+// the patch centre, so the FP32 residual keeps its precision however far the
+// ray origin is from the patch.  The method is the reference's
+// (BezierPatchOps::newtonRhapson, src/math/bezier_patch.h:197-266); only the
+// coordinate origin and the evaluation scheme differ.
+#pragma once
+
+#include <cstdint>
+
+namespace nrt {
+namespace dev {
+
+constexpr int kMaxDeg = 7;
+
+__host__ __device__ constexpr int padded_points(int p, int q) { return (((p + 1) * (q + 1)) + 3) & ~3; }
+
+__device__ __forceinline__ float fmx(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmx(double a, double b, double c) { return ::fma(a, b, c); }
+
+// Packed patch header: x = first float of the SoA block, y = p | q<<4 |
+// flags<<8, z = global patch id, w = surface id.
+enum : int { kFlagPositiveWeights = 1 };
+
+struct RayFrame {
+    float ox, oy, oz, dx, dy, dz;
+    float n1x, n1y, n1z, n2x, n2y, n2z;
+};
+
+// Per (ray, patch) offsets, FP32 for the iteration and FP64 for the final step.
+struct PatchRay {
+    float e1, e2, tc;
+    double e1d, e2d, tcd;
+};
+
+struct NewtonOpts {
+    int max_iter;
+    float eps;
+    float det_eps;
+    float cond_fp64;
+    int fp64_final;
+};
+
+struct NewtonOut {
+    int evals;       // > 0 converged after this many evaluations; < 0 not converged
+    float u, v;
+    float t;         // along the ray, in units of |d|
+    float sx, sy, sz, ux, uy, uz, vx, vy, vz;  // S (local), dS/du, dS/dv
+    int fp64_solves;
+    int fp64_final;
+};
+
+// PCG hash (src/math/math_utils.h:12-17).
+__device__ __forceinline__ uint32_t pcg_hash(uint32_t x) {
+    x = x * 747796405u + 2891336453u;
+    const uint32_t w = ((x >> ((x >> 28u) + 4u)) ^ x) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+
+// The two planes containing the ray, getRayPlanes (math_utils.h:33-54) with
+// IEEE square root and division.
+__device__ __forceinline__ void ray_planes(RayFrame& r) {
+    const float ax = fabsf(r.dx), ay = fabsf(r.dy), az = fabsf(r.dz);
+    const bool xdom = (ax > ay) && (ax > az);
+    const float bx = xdom ? r.dx : r.dy, by = xdom ? r.dy : r.dz;
+    const float rl = __frcp_rn(__fsqrt_rn(bx * bx + by * by));
+    if (xdom) { r.n1x = r.dy * rl; r.n1y = -r.dx * rl; r.n1z = 0.f; }
+    else { r.n1x = 0.f; r.n1y = r.dz * rl; r.n1z = -r.dy * rl; }
+    const float il = __frcp_rn(__fsqrt_rn(r.dx * r.dx + r.dy * r.dy + r.dz * r.dz));
+    const float ux = r.dx * il, uy = r.dy * il, uz = r.dz * il;
+    r.n2x = r.n1y * uz - r.n1z * uy;
+    r.n2y = r.n1z * ux - r.n1x * uz;
+    r.n2z = r.n1x * uy - r.n1y * ux;
+}
+
+__device__ __forceinline__ PatchRay patch_ray(const RayFrame& r, double cx, double cy, double cz) {
+    const double ox = (double)r.ox - cx, oy = (double)r.oy - cy, oz = (double)r.oz - cz;
+    PatchRay pr;
+    pr.e1d = -((double)r.n1x * ox + (double)r.n1y * oy + (double)r.n1z * oz);
+    pr.e2d = -((double)r.n2x * ox + (double)r.n2y * oy + (double)r.n2z * oz);
+    pr.tcd = -((double)r.dx * ox + (double)r.dy * oy + (double)r.dz * oz);
+    pr.e1 = (float)pr.e1d;
+    pr.e2 = (float)pr.e2d;
+    pr.tc = (float)pr.tcd;
+    return pr;
+}
+
+// Tensor-product rational Bezier evaluation of one homogeneous coordinate:
+// every row (along v) is reduced by de Casteljau to two points, giving the
+// row point at v and its v-derivative; the row points are reduced along u to
+// two points (value and u-derivative) and the v-derivatives to one point.
+// This yields H, dH/du, dH/dv with (p+1)q(q+1)/2 + p(p+1) lerps, against the
+// two full passes of BezierPatchEval (src/math/bezier_patch.h:172-191).
+template <int P, int Q, class T>
+__device__ __forceinline__ void eval_coord(const T (&c)[(P + 1) * (Q + 1)], T u, T v, T& h, T& hu, T& hv) {
+    T pt[P + 1], dv[P + 1];
+#pragma unroll
+    for (int i = 0; i <= P; ++i) {
+        T r[Q + 1];
+#pragma unroll
+        for (int j = 0; j <= Q; ++j) r[j] = c[i * (Q + 1) + j];
+#pragma unroll
+        for (int k = 1; k < Q; ++k)
+#pragma unroll
+            for (int j = 0; j <= Q - k; ++j) r[j] = fmx(v, r[j + 1] - r[j], r[j]);
+        const T dl = r[1] - r[0];
+        pt[i] = fmx(v, dl, r[0]);
+        dv[i] = T(Q) * dl;
+    }
+#pragma unroll
+    for (int k = 1; k < P; ++k)
+#pragma unroll
+        for (int i = 0; i <= P - k; ++i) pt[i] = fmx(u, pt[i + 1] - pt[i], pt[i]);
+#pragma unroll
+    for (int k = 1; k <= P; ++k)
+#pragma unroll
+        for (int i = 0; i <= P - k; ++i) dv[i] = fmx(u, dv[i + 1] - dv[i], dv[i]);
+    const T dl = pt[1] - pt[0];
+    h = fmx(u, dl, pt[0]);
+    hu = T(P) * dl;
+    hv = dv[0];
+}
+
+// Load one coordinate array of a patch block with 16-byte loads.
+template <int P, int Q, class T>
+__device__ __forceinline__ void load_coord(const float* __restrict__ src, T (&c)[(P + 1) * (Q + 1)]) {
+    constexpr int N = (P + 1) * (Q + 1);
+    constexpr int NP = padded_points(P, Q);
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int k = 0; k < NP / 4; ++k) {
+        const float4 f = __ldg(s4 + k);
+        if (4 * k + 0 < N) c[4 * k + 0] = (T)f.x;
+        if (4 * k + 1 < N) c[4 * k + 1] = (T)f.y;
+        if (4 * k + 2 < N) c[4 * k + 2] = (T)f.z;
+        if (4 * k + 3 < N) c[4 * k + 3] = (T)f.w;
+    }
+}
+
+template <int P, int Q, class T>
+__device__ __forceinline__ void eval_patch(const float* __restrict__ blk, T u, T v, T (&H)[4], T (&Hu)[4],
+                                           T (&Hv)[4]) {
+    constexpr int NP = padded_points(P, Q);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        T c[(P + 1) * (Q + 1)];
+        load_coord<P, Q, T>(blk + a * NP, c);
+        eval_coord<P, Q, T>(c, u, v, H[a], Hu[a], Hv[a]);
+    }
+}
+
+// FP64 evaluation that streams one row at a time from memory, so that high
+// degrees do not hold a whole coordinate array in (double) registers.
+template <int P, int Q>
+__device__ __forceinline__ void eval_patch_fp64(const float* __restrict__ blk, double u, double v, double (&H)[4],
+                                                double (&Hu)[4], double (&Hv)[4]) {
+    constexpr int NP = padded_points(P, Q);
+#pragma unroll 1
+    for (int a = 0; a < 4; ++a) {
+        const float* __restrict__ src = blk + a * NP;
+        double pt[P + 1], dv[P + 1];
+#pragma unroll
+        for (int i = 0; i <= P; ++i) {
+            double r[Q + 1];
+#pragma unroll
+            for (int j = 0; j <= Q; ++j) r[j] = (double)__ldg(src + i * (Q + 1) + j);
+#pragma unroll
+            for (int k = 1; k < Q; ++k)
+#pragma unroll
+                for (int j = 0; j <= Q - k; ++j) r[j] = fmx(v, r[j + 1] - r[j], r[j]);
+            const double dl = r[1] - r[0];
+            pt[i] = fmx(v, dl, r[0]);
+            dv[i] = double(Q) * dl;
+        }
+#pragma unroll
+        for (int k = 1; k < P; ++k)
+#pragma unroll
+            for (int i = 0; i <= P - k; ++i) pt[i] = fmx(u, pt[i + 1] - pt[i], pt[i]);
+#pragma unroll
+        for (int k = 1; k <= P; ++k)
+#pragma unroll
+            for (int i = 0; i <= P - k; ++i) dv[i] = fmx(u, dv[i + 1] - dv[i], dv[i]);
+        const double dl = pt[1] - pt[0];
+        H[a] = fmx(u, dl, pt[0]);
+        Hu[a] = double(P) * dl;
+        Hv[a] = dv[0];
+    }
+}
+
+// Ray-space hull test.  For w > 0 the surface point S(u,v), u,v in [0,1], is
+// a convex combination of the dehomogenised control points, so the plane
+// residual n.S + e is bounded by the control points' residuals.  If every
+// control point lies beyond +lim (or below -lim) for either plane, no
+// evaluation can meet |r1| + |r2| < eps and Newton's outcome is "no hit":
+// the test can be skipped without changing the result.  lim = eps plus a
+// rounding margin scaled by the patch radius.
+template <int P, int Q>
+__device__ __forceinline__ bool hull_misses(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                            float lim) {
+    constexpr int N = (P + 1) * (Q + 1);
+    constexpr int NP = padded_points(P, Q);
+    const float4* X = reinterpret_cast<const float4*>(blk);
+    const float4* Y = reinterpret_cast<const float4*>(blk + NP);
+    const float4* Z = reinterpret_cast<const float4*>(blk + 2 * NP);
+    const float4* W = reinterpret_cast<const float4*>(blk + 3 * NP);
+    bool pos1 = true, neg1 = true, pos2 = true, neg2 = true;
+#pragma unroll
+    for (int k = 0; k < NP / 4; ++k) {
+        const float4 x = __ldg(X + k), y = __ldg(Y + k), z = __ldg(Z + k), w = __ldg(W + k);
+        const float xs[4] = {x.x, x.y, x.z, x.w}, ys[4] = {y.x, y.y, y.z, y.w};
+        const float zs[4] = {z.x, z.y, z.z, z.w}, ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            if (4 * k + l >= N) break;
+            const float a = fmaf(r.n1x, xs[l], fmaf(r.n1y, ys[l], fmaf(r.n1z, zs[l], pr.e1 * ws[l])));
+            const float b = fmaf(r.n2x, xs[l], fmaf(r.n2y, ys[l], fmaf(r.n2z, zs[l], pr.e2 * ws[l])));
+            const float m = lim * ws[l];
+            pos1 &= a > m;
+            neg1 &= a < -m;
+            pos2 &= b > m;
+            neg2 &= b < -m;
+        }
+    }
+    return pos1 | neg1 | pos2 | neg2;
+}
+
+// One FP64 Newton step from a converged (u, v): evaluate in double, solve the
+// 2x2 system exactly in double, clamp, and move S to first order.
+template <int P, int Q>
+__device__ __forceinline__ void final_step_fp64(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                                NewtonOut& o) {
+    double H[4], Hu[4], Hv[4];
+    eval_patch_fp64<P, Q>(blk, (double)o.u, (double)o.v, H, Hu, Hv);
+    const double iw = 1.0 / H[3];
+    const double S[3] = {H[0] * iw, H[1] * iw, H[2] * iw};
+    double Su[3], Sv[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        Su[a] = (Hu[a] - S[a] * Hu[3]) * iw;
+        Sv[a] = (Hv[a] - S[a] * Hv[3]) * iw;
+    }
+    const double n1[3] = {r.n1x, r.n1y, r.n1z}, n2[3] = {r.n2x, r.n2y, r.n2z};
+    const double r1 = n1[0] * S[0] + n1[1] * S[1] + n1[2] * S[2] + pr.e1d;
+    const double r2 = n2[0] * S[0] + n2[1] * S[1] + n2[2] * S[2] + pr.e2d;
+    const double j11 = n1[0] * Su[0] + n1[1] * Su[1] + n1[2] * Su[2];
+    const double j21 = n2[0] * Su[0] + n2[1] * Su[1] + n2[2] * Su[2];
+    const double j12 = n1[0] * Sv[0] + n1[1] * Sv[1] + n1[2] * Sv[2];
+    const double j22 = n2[0] * Sv[0] + n2[1] * Sv[1] + n2[2] * Sv[2];
+    const double det = j11 * j22 - j12 * j21;
+    double du = 0.0, dv = 0.0;
+    if (det != 0.0) {
+        du = (j22 * r1 - j12 * r2) / det;
+        dv = (j11 * r2 - j21 * r1) / det;
+    }
+    const double un = fmin(fmax((double)o.u - du, 0.0), 1.0), vn = fmin(fmax((double)o.v - dv, 0.0), 1.0);
+    const double su = un - (double)o.u, sv = vn - (double)o.v;
+    double Sn[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Sn[a] = S[a] + Su[a] * su + Sv[a] * sv;
+    const double d[3] = {r.dx, r.dy, r.dz};
+    const double t = Sn[0] * d[0] + Sn[1] * d[1] + Sn[2] * d[2] + pr.tcd;
+    o.u = (float)un;
+    o.v = (float)vn;
+    o.t = (float)t;
+    o.sx = (float)Sn[0]; o.sy = (float)Sn[1]; o.sz = (float)Sn[2];
+    o.ux = (float)Su[0]; o.uy = (float)Su[1]; o.uz = (float)Su[2];
+    o.vx = (float)Sv[0]; o.vy = (float)Sv[1]; o.vz = (float)Sv[2];
+    o.fp64_final = 1;
+}
+
+// Newton-Raphson on F(u,v) = (n1.S + e1, n2.S + e2) from (u0, v0); the
+// iteration, thresholds, seeded pull on a singular Jacobian and clamping follow
+// BezierPatchOps::newtonRhapson (src/math/bezier_patch.h:197-266).  When
+// cond_fp64 > 0 and ||J||_F^2 / |det J| exceeds it, the 2x2 solve is done in
+// FP64 (products of floats are exact there, so det J has no cancellation).
+template <int P, int Q>
+__device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                            float u0, float v0, uint32_t seed, const NewtonOpts& op) {
+    NewtonOut o;
+    o.fp64_solves = 0;
+    o.fp64_final = 0;
+    float u = u0, v = v0;
+    for (int it = 1; it <= op.max_iter; ++it) {
+        float H[4], Hu[4], Hv[4];
+        eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
+        const float iw = __frcp_rn(H[3]);
+        const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
+        const float ux = (Hu[0] - sx * Hu[3]) * iw, uy = (Hu[1] - sy * Hu[3]) * iw, uz = (Hu[2] - sz * Hu[3]) * iw;
+        const float vx = (Hv[0] - sx * Hv[3]) * iw, vy = (Hv[1] - sy * Hv[3]) * iw, vz = (Hv[2] - sz * Hv[3]) * iw;
+        const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
+        const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
+        if (fabsf(r1) + fabsf(r2) < op.eps) {
+            o.evals = it;
+            o.u = u; o.v = v;
+            o.sx = sx; o.sy = sy; o.sz = sz;
+            o.ux = ux; o.uy = uy; o.uz = uz;
+            o.vx = vx; o.vy = vy; o.vz = vz;
+            o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
+            if (op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+            return o;
+        }
+        const float j11 = r.n1x * ux + r.n1y * uy + r.n1z * uz;
+        const float j21 = r.n2x * ux + r.n2y * uy + r.n2z * uz;
+        const float j12 = r.n1x * vx + r.n1y * vy + r.n1z * vz;
+        const float j22 = r.n2x * vx + r.n2y * vy + r.n2z * vz;
+        seed = pcg_hash(seed);
+        const float rnd1 = (float)seed * 2.3283064e-10f;
+        seed = pcg_hash(seed);
+        const float rnd2 = (float)seed * 2.3283064e-10f;
+        const float det = j11 * j22 - j12 * j21;
+        if (fabsf(det) < op.det_eps) {
+            u = u + 0.1f * ((u0 - u) * rnd1);
+            v = v + 0.1f * ((v0 - v) * rnd2);
+        } else if (op.cond_fp64 > 0.f &&
+                   (j11 * j11 + j12 * j12 + j21 * j21 + j22 * j22) > op.cond_fp64 * fabsf(det)) {
+            const double dd = (double)j11 * j22 - (double)j12 * j21;
+            u = (float)((double)u - ((double)j22 * r1 - (double)j12 * r2) / dd);
+            v = (float)((double)v - ((double)j11 * r2 - (double)j21 * r1) / dd);
+            ++o.fp64_solves;
+        } else {
+            const float id = __frcp_rn(det);
+            u = u - (j22 * r1 - j12 * r2) * id;
+            v = v - (j11 * r2 - j21 * r1) * id;
+        }
+        u = fminf(fmaxf(u, 0.f), 1.f);
+        v = fminf(fmaxf(v, 0.f), 1.f);
+    }
+    o.evals = -op.max_iter;
+    o.u = u; o.v = v;
+    return o;
+}
+
+// The reference's ray/bilinear-patch guess through the four corners
+// (BezierPatchOps::biliniearRay, src/math/bezier_patch.h:272-327), computed in
+// world coordinates with round-to-nearest products and sums that are never
+// fused, so it reproduces the reference's host arithmetic exactly.  As written
+// there, n.pb and n.d vanish up to rounding (n = d x pb), so the guess is
+// (0.5, 0.5) unless that rounding noise selects a root.
+__device__ __forceinline__ void bilinear_guess(const float4* __restrict__ cr, const RayFrame& r, float& gu,
+                                               float& gv) {
+#define M_(a, b) __fmul_rn(a, b)
+#define A_(a, b) __fadd_rn(a, b)
+#define S_(a, b) __fsub_rn(a, b)
+    const float4 c00 = __ldg(cr), c10 = __ldg(cr + 1), c11 = __ldg(cr + 2), c01 = __ldg(cr + 3);
+    float e10[3] = {S_(c10.x, c00.x), S_(c10.y, c00.y), S_(c10.z, c00.z)};
+    float e11[3] = {S_(c11.x, c10.x), S_(c11.y, c10.y), S_(c11.z, c10.z)};
+    float e00[3] = {S_(c01.x, c00.x), S_(c01.y, c00.y), S_(c01.z, c00.z)};
+    float w[3] = {S_(c01.x, c11.x), S_(c01.y, c11.y), S_(c01.z, c11.z)};
+    auto cross = [](const float* a, const float* b, float* o) {
+        o[0] = S_(M_(a[1], b[2]), M_(a[2], b[1]));
+        o[1] = S_(M_(a[2], b[0]), M_(a[0], b[2]));
+        o[2] = S_(M_(a[0], b[1]), M_(a[1], b[0]));
+    };
+    auto dot = [](const float* a, const float* b) { return A_(A_(M_(a[0], b[0]), M_(a[1], b[1])), M_(a[2], b[2])); };
+    float qn[3];
+    cross(e10, w, qn);
+    const float d[3] = {r.dx, r.dy, r.dz};
+    float q00[3] = {S_(c00.x, r.ox), S_(c00.y, r.oy), S_(c00.z, r.oz)};
+    float q10[3] = {S_(c10.x, r.ox), S_(c10.y, r.oy), S_(c10.z, r.oz)};
+    float t0[3], t1[3];
+    cross(q00, d, t0);
+    cross(q10, d, t1);
+    const float a = dot(t0, e00), c = dot(qn, d);
+    float b = dot(t1, e11);
+    b = S_(b, A_(a, c));
+    float det = S_(M_(b, b), M_(M_(4.0f, a), c));
+    gu = 0.5f;
+    gv = 0.5f;
+    if (det < 0.f) return;
+    det = __fsqrt_rn(det);
+    float ux[2];
+    if (c == 0.f) { ux[0] = __fdiv_rn(-a, b); ux[1] = -1.f; }
+    else {
+        ux[0] = __fdiv_rn(S_(-b, copysignf(det, b)), 2.0f);
+        ux[1] = __fdiv_rn(a, ux[0]);
+        ux[0] = __fdiv_rn(ux[0], c);
+    }
+    float best = INFINITY;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        if (ux[i] < 0.f || ux[i] > 1.f) continue;
+        const float om = S_(1.0f, ux[i]);
+        const float pb[3] = {A_(M_(e00[0], om), M_(e11[0], ux[i])), A_(M_(e00[1], om), M_(e11[1], ux[i])),
+                             A_(M_(e00[2], om), M_(e11[2], ux[i]))};
+        float n[3];
+        cross(d, pb, n);
+        const float dd = dot(n, n), tx = dot(n, pb), vx = dot(n, d);
+        if (tx > 0.f && 0.f <= vx && vx <= dd && tx < best) {
+            gu = ux[i];
+            gv = __fdiv_rn(vx, dd);
+            best = tx;
+        }
+    }
+#undef M_
+#undef A_
+#undef S_
+}
+
+// Slab test returning the entry distance (tmin starts at 0) or +inf, as
+// BoundsOps::intersectBound (src/math/bounds_ops.h:83-114).
+__device__ __forceinline__ float slab(float lox, float loy, float loz, float hix, float hiy, float hiz,
+                                      const RayFrame& r, float rdx, float rdy, float rdz) {
+    const float t0x = (lox - r.ox) * rdx, t1x = (hix - r.ox) * rdx;
+    const float t0y = (loy - r.oy) * rdy, t1y = (hiy - r.oy) * rdy;
+    const float t0z = (loz - r.oz) * rdz, t1z = (hiz - r.oz) * rdz;
+    const float lo = fmaxf(fminf(t0z, t1z), fmaxf(fminf(t0y, t1y), fmaxf(fminf(t0x, t1x), 0.f)));
+    const float hi = fminf(fmaxf(t0z, t1z), fminf(fmaxf(t0y, t1y), fmaxf(t0x, t1x)));
+    return (lo <= hi && hi > 0.f) ? lo : INFINITY;
+}
+
+}  // namespace dev
+}  // namespace nrt

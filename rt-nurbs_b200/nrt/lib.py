@@ -1,0 +1,291 @@
+"""ctypes declarations of include/nrt.h and thin Python wrappers."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))  # rt-nurbs_b200/
+_LIB = None
+
+INIT_MIDPOINT, INIT_BILINEAR, INIT_LEARNED = 0, 1, 2
+SCHED_PIXEL, SCHED_WAVEFRONT = 0, 1
+BVH_BINNED_SAH, BVH_EXACT_SAH = 0, 1
+
+
+class NrtError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"nrt error {status}: {msg}")
+        self.status = status
+
+
+class NurbsSurface(C.Structure):
+    _fields_ = [("control_points", C.c_void_p), ("u_knots", C.c_void_p), ("v_knots", C.c_void_p),
+                ("n", C.c_int), ("m", C.c_int), ("p", C.c_int), ("q", C.c_int)]
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("builder", C.c_int), ("max_leaf", C.c_int), ("device", C.c_int)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("n_patches", C.c_int), ("n_surfaces", C.c_int), ("n_nodes", C.c_int), ("bvh_depth", C.c_int),
+                ("device_bytes", C.c_size_t), ("degree_hist", C.c_int * 64)]
+
+
+class RaysC(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("ox", "oy", "oz", "dx", "dy", "dz")]
+
+
+class HitsC(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("patch", "t", "u", "v", "iters", "tests", "geom")]
+
+
+class IntersectOpts(C.Structure):
+    _fields_ = [("init_mode", C.c_int), ("max_iter", C.c_int), ("eps", C.c_float), ("det_eps", C.c_float),
+                ("cond_fp64", C.c_float), ("fp64_final", C.c_int), ("hull_cull", C.c_int), ("schedule", C.c_int),
+                ("seed_offset", C.c_int), ("flat_threshold", C.c_float), ("cam_k", C.c_float)]
+
+    def replace(self, **kw) -> "IntersectOpts":
+        o = IntersectOpts()
+        C.pointer(o)[0] = self
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_COUNTER_NAMES = ("rays", "box_tests", "patch_candidates", "patch_culled", "newton_solves", "newton_evals",
+                  "fp64_solves", "fp64_final_steps", "hits", "errors")
+
+
+class Counters(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in _COUNTER_NAMES] + [("evals_by_degree", C.c_uint64 * 64),
+                                                            ("hull_tests_by_degree", C.c_uint64 * 64)]
+
+    def as_dict(self) -> dict:
+        d = {k: int(getattr(self, k)) for k in _COUNTER_NAMES}
+        d["evals_by_degree"] = {(k // 8, k % 8): int(v) for k, v in enumerate(self.evals_by_degree) if v}
+        d["hull_tests_by_degree"] = {(k // 8, k % 8): int(v) for k, v in enumerate(self.hull_tests_by_degree) if v}
+        return d
+
+
+class CameraC(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("look", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float),
+                ("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("seed", C.c_uint32)]
+
+
+def lib_path() -> str:
+    return os.path.join(PKG, "lib", "libnrt.so")
+
+
+def lib():
+    """Load libnrt.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise NrtError(-1, f"{path} is missing: build it with `make -C rt-nurbs_b200` (or __graft_entry__.build())")
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.nrt_last_error.restype = C.c_char_p
+        L.nrt_version.restype = C.c_char_p
+        L.nrt_decompose_count.argtypes = [C.POINTER(NurbsSurface), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.nrt_decompose.argtypes = [C.POINTER(NurbsSurface), vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.nrt_patch_bounds.argtypes = [vp, vp, vp, C.c_int, vp]
+        L.nrt_build_bvh_binary.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, C.POINTER(C.c_int)]
+        L.nrt_scene_create.argtypes = [C.POINTER(NurbsSurface), C.c_int, C.POINTER(BuildOpts), C.POINTER(vp)]
+        L.nrt_scene_create_from_patches.argtypes = [vp, vp, vp, C.c_int, C.POINTER(BuildOpts), C.POINTER(vp)]
+        L.nrt_scene_destroy.argtypes = [vp]
+        L.nrt_scene_get_info.argtypes = [vp, C.POINTER(SceneInfo)]
+        L.nrt_scene_patch_table.argtypes = [vp, vp, vp]
+        L.nrt_default_opts.argtypes = [C.POINTER(IntersectOpts)]
+        L.nrt_default_opts.restype = None
+        L.nrt_reference_opts.argtypes = [C.POINTER(IntersectOpts)]
+        L.nrt_reference_opts.restype = None
+        L.nrt_intersect.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts), C.POINTER(HitsC), vp]
+        L.nrt_enable_counters.argtypes = [vp, C.c_int]
+        L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
+        L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
+        _LIB = L
+    return _LIB
+
+
+def _check(status: int):
+    if status != 0:
+        raise NrtError(status, lib().nrt_last_error().decode())
+
+
+def default_opts(**kw) -> IntersectOpts:
+    o = IntersectOpts()
+    lib().nrt_default_opts(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def reference_opts(**kw) -> IntersectOpts:
+    o = IntersectOpts()
+    lib().nrt_reference_opts(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _surface_struct(s):
+    cp = np.ascontiguousarray(s.cp, np.float32)
+    U = np.ascontiguousarray(s.U, np.float32)
+    V = np.ascontiguousarray(s.V, np.float32)
+    st = NurbsSurface(cp.ctypes.data, U.ctypes.data, V.ctypes.data, s.n, s.m, s.p, s.q)
+    return st, (cp, U, V)
+
+
+def decompose(s):
+    """Host decomposition of one surface: (cp (P,4) float32, ranges (N,4), (nbU, nbV))."""
+    L = lib()
+    st, keep = _surface_struct(s)
+    nu, nv = C.c_int(), C.c_int()
+    _check(L.nrt_decompose_count(C.byref(st), C.byref(nu), C.byref(nv)))
+    N = nu.value * nv.value
+    cp = np.zeros((N * (s.p + 1) * (s.q + 1), 4), np.float32)
+    ranges = np.zeros((N, 4), np.float32)
+    _check(L.nrt_decompose(C.byref(st), cp.ctypes.data, ranges.ctypes.data, C.byref(nu), C.byref(nv)))
+    return cp, ranges, (nu.value, nv.value)
+
+
+def patch_bounds(cp, off, deg) -> np.ndarray:
+    cp = np.ascontiguousarray(cp, np.float32)
+    off = np.ascontiguousarray(off, np.int32)
+    deg = np.ascontiguousarray(deg, np.int32)
+    out = np.zeros((off.shape[0], 6), np.float32)
+    _check(lib().nrt_patch_bounds(cp.ctypes.data, off.ctypes.data, deg.ctypes.data, off.shape[0], out.ctypes.data))
+    return out
+
+
+def build_bvh_binary(boxes, builder=BVH_EXACT_SAH):
+    boxes = np.ascontiguousarray(boxes, np.float32)
+    N = boxes.shape[0]
+    M = 2 * N - 1
+    nb = np.zeros((M, 6), np.float32)
+    lf = np.zeros(M, np.uint32)
+    cnt = np.zeros(M, np.uint32)
+    order = np.zeros(N, np.int32)
+    used = C.c_int()
+    _check(lib().nrt_build_bvh_binary(boxes.ctypes.data, N, builder, nb.ctypes.data, lf.ctypes.data,
+                                      cnt.ctypes.data, order.ctypes.data, C.byref(used)))
+    return nb, lf, cnt, order, used.value
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class Scene:
+    """A device scene (decomposition + BVH + upload), nrt_scene_create."""
+
+    def __init__(self, surfaces=None, patches=None, builder=BVH_BINNED_SAH, max_leaf=1, device=0):
+        L = lib()
+        self._h = C.c_void_p()
+        opts = BuildOpts(builder, max_leaf, device)
+        if surfaces is not None:
+            arr = (NurbsSurface * len(surfaces))()
+            keep = []
+            for i, s in enumerate(surfaces):
+                st, k = _surface_struct(s)
+                arr[i] = st
+                keep.append(k)
+            _check(L.nrt_scene_create(arr, len(surfaces), C.byref(opts), C.byref(self._h)))
+        else:
+            cp, off, deg = (np.ascontiguousarray(patches[0], np.float32), np.ascontiguousarray(patches[1], np.int32),
+                            np.ascontiguousarray(patches[2], np.int32))
+            _check(L.nrt_scene_create_from_patches(cp.ctypes.data, off.ctypes.data, deg.ctypes.data, off.shape[0],
+                                                   C.byref(opts), C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().nrt_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        inf = SceneInfo()
+        _check(lib().nrt_scene_get_info(self._h, C.byref(inf)))
+        hist = {(k // 8, k % 8): int(v) for k, v in enumerate(inf.degree_hist) if v}
+        return {"n_patches": inf.n_patches, "n_surfaces": inf.n_surfaces, "n_nodes": inf.n_nodes,
+                "bvh_depth": inf.bvh_depth, "device_bytes": int(inf.device_bytes), "degree_hist": hist}
+
+    def patch_table(self):
+        n = self.info()["n_patches"]
+        surf = np.zeros(n, np.int32)
+        ranges = np.zeros((n, 4), np.float32)
+        _check(lib().nrt_scene_patch_table(self._h, surf.ctypes.data, ranges.ctypes.data))
+        return surf, ranges
+
+    def enable_counters(self, on=True):
+        _check(lib().nrt_enable_counters(self._h, int(on)))
+
+    def counters(self, stream=None) -> dict:
+        c = Counters()
+        _check(lib().nrt_get_counters(self._h, C.byref(c), _stream_ptr(stream)))
+        return c.as_dict()
+
+    def intersect(self, rays, opts: IntersectOpts | None = None, out=None, stream=None, geom=False, extra=True):
+        """rays: 6 float32 CUDA tensors (ox, oy, oz, dx, dy, dz).  Returns a dict of CUDA tensors."""
+        import torch
+
+        if opts is None:
+            opts = default_opts()
+        n = rays[0].numel()
+        dev = rays[0].device
+        if out is None:
+            out = {"patch": torch.empty(n, dtype=torch.int32, device=dev),
+                   "t": torch.empty(n, dtype=torch.float32, device=dev),
+                   "u": torch.empty(n, dtype=torch.float32, device=dev),
+                   "v": torch.empty(n, dtype=torch.float32, device=dev)}
+            if extra:
+                out["iters"] = torch.empty(n, dtype=torch.int32, device=dev)
+                out["tests"] = torch.empty(n, dtype=torch.int32, device=dev)
+            if geom:
+                out["geom"] = torch.empty((n, 9), dtype=torch.float32, device=dev)
+        r = RaysC(*[C.c_void_p(a.data_ptr()) for a in rays])
+        h = HitsC(_ptr(out["patch"]), _ptr(out["t"]), _ptr(out["u"]), _ptr(out["v"]), _ptr(out.get("iters")),
+                  _ptr(out.get("tests")), _ptr(out.get("geom")))
+        _check(lib().nrt_intersect(self._h, C.byref(r), n, C.byref(opts), C.byref(h), _stream_ptr(stream)))
+        return out
+
+
+class Camera(CameraC):
+    pass
+
+
+def camera_rays(cam, device="cuda", stream=None):
+    """Primary rays for a scenes.Camera as 6 CUDA tensors."""
+    import torch
+
+    c = CameraC((C.c_float * 3)(*cam.eye), (C.c_float * 3)(*cam.look), (C.c_float * 3)(*cam.up), cam.fov_deg,
+                cam.width, cam.height, cam.spp, cam.seed)
+    n = cam.width * cam.height * cam.spp
+    arrs = [torch.empty(n, dtype=torch.float32, device=device) for _ in range(6)]
+    r = RaysC(*[C.c_void_p(a.data_ptr()) for a in arrs])
+    _check(lib().nrt_generate_camera_rays(C.byref(c), C.byref(r), _stream_ptr(stream)))
+    return arrs

@@ -180,23 +180,33 @@ def random_surface(rng, centre, deg_range=(2, 5), net_range=(16, 32), relief: fl
 
 
 def surfaces_grid_scene(n_surfaces: int, seed: int, width: int, height: int, spp: int, relief: float = 1.0,
-                        deg_range=(2, 5), net_range=(16, 32), spacing: float = 1.5, name: str = "surfaces") -> Scene:
-    """n_surfaces random surfaces (see random_surface) on a square grid in the
-    z=0 plane with the given spacing, seen by a camera above and in front of the
-    grid at 45 degrees elevation whose view covers the grid."""
+                        deg_range=(2, 5), net_range=(16, 32), spacing: float = 1.0, layers: int = 4,
+                        name: str = "surfaces") -> Scene:
+    """n_surfaces random surfaces (see random_surface) whose boxes sit on a
+    lattice of `layers` levels with the given spacing (64 -> 4x4x4,
+    256 -> 8x8x4), so that most camera rays cross several surfaces.  The camera
+    looks at the lattice centre from the direction (1, -1.3, 0.8), close
+    enough (0.55x the distance at which the lattice's bounding sphere would
+    just fit the short image axis) that the lattice fills the frame."""
     rng = np.random.default_rng(seed)
-    side = int(np.ceil(np.sqrt(n_surfaces)))
-    half = 0.5 * spacing * (side - 1)
+    layers = max(1, min(layers, n_surfaces))
+    per_layer = int(np.ceil(n_surfaces / layers))
+    side = int(np.ceil(np.sqrt(per_layer)))
+    dims = np.array([side, int(np.ceil(per_layer / side)), layers], np.float64)
+    half = 0.5 * spacing * (dims - 1)
     surfs = []
     for k in range(n_surfaces):
-        cx = -half + spacing * (k % side)
-        cy = -half + spacing * (k // side)
-        surfs.append(random_surface(rng, (cx, cy, 0.0), deg_range, net_range, relief))
-    extent = half + 0.9
-    dist = 1.55 * extent / np.tan(np.radians(30.0))
-    eye = (0.0, -dist * np.cos(np.radians(45.0)), dist * np.sin(np.radians(45.0)))
-    cam = Camera(eye, (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 60.0, width, height, spp, seed)
-    return Scene(name, surfs, cam, {"side": side, "spacing": spacing, "relief": relief})
+        ix, iy, iz = k % side, (k // side) % int(dims[1]), k // per_layer
+        centre = (-half[0] + spacing * ix, -half[1] + spacing * iy, -half[2] + spacing * iz)
+        surfs.append(random_surface(rng, centre, deg_range, net_range, relief))
+    radius = float(np.linalg.norm(half + 0.5 * spacing))
+    fov = 60.0
+    dist = 0.55 * radius / np.sin(np.radians(fov / 2.0))
+    view = np.array([1.0, -1.3, 0.8])
+    view /= np.linalg.norm(view)
+    eye = tuple(float(x) for x in dist * view)
+    cam = Camera(eye, (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), fov, width, height, spp, seed)
+    return Scene(name, surfs, cam, {"lattice": dims.astype(int).tolist(), "spacing": spacing, "relief": relief})
 
 
 def mixed_degree_scene(seed: int = 1, width: int = 1920, height: int = 1080, spp: int = 4) -> Scene:

@@ -1,0 +1,139 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol of
+include/nrt.h, and its host-side pipeline (decomposition, patch bounds, BVH
+builders) matches the reference's outputs in the golden fixtures."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_surfaces, load_golden
+
+FIXTURES = ["heightfield", "torus", "sphere", "mixed4"]
+
+
+@pytest.fixture(scope="module")
+def nrt_mod():
+    import nrt
+
+    nrt.lib()
+    return nrt
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "nrt.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(nrt_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_header(nrt_mod):
+    import ctypes
+
+    L = ctypes.CDLL(nrt_mod.lib_path())
+    syms = header_symbols()
+    assert len(syms) >= 15
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_version_and_opts(nrt_mod):
+    assert b"nrt" in nrt_mod.lib().nrt_version()
+    d = nrt_mod.default_opts()
+    assert (d.init_mode, d.max_iter, d.eps, d.hull_cull) == (0, 8, np.float32(1e-6), 0)
+    r = nrt_mod.reference_opts()
+    assert (r.init_mode, r.max_iter, r.eps) == (1, 7, np.float32(1e-4))
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_decompose_bit_exact_vs_reference(nrt_mod, name):
+    g = load_golden(name)
+    for k, s in enumerate(golden_surfaces(g)):
+        cp, ranges, _ = nrt_mod.decompose(s)
+        assert np.array_equal(cp.view(np.uint32), g[f"surf{k}_patch_cp"].view(np.uint32))
+        assert np.array_equal(ranges, g[f"surf{k}_patch_ranges"])
+
+
+def test_decompose_high_degree(nrt_mod, oracle_mod):
+    """Degrees above the reference's cap of 4 (up to 7) decompose and agree
+    with the oracle restatement bit for bit."""
+    from nrt import scenes
+
+    for p, q in [(5, 5), (7, 6), (6, 7), (7, 7), (1, 7), (2, 1)]:
+        rng = np.random.default_rng(p * 10 + q)
+        n, m = p + 5, q + 4
+        cp = np.empty(((n + 1) * (m + 1), 4), np.float32)
+        cp[:, :3] = rng.normal(size=((n + 1) * (m + 1), 3))
+        cp[:, 3] = rng.uniform(0.5, 2.0, (n + 1) * (m + 1))
+        cp[:, :3] *= cp[:, 3:]
+        s = scenes.Surface(cp, scenes._random_knots(rng, n, p), scenes._random_knots(rng, m, q), n, m, p, q)
+        cpn, ranges, (nu, nv) = nrt_mod.decompose(s)
+        ocp, _, orng, (onu, onv) = oracle_mod.decompose(s, f64=False)
+        assert (nu, nv) == (onu, onv) and nu * nv > 1
+        assert np.array_equal(cpn.view(np.uint32), ocp.view(np.uint32))
+        assert np.array_equal(ranges, orng)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_bounds_and_exact_bvh_vs_reference(nrt_mod, oracle_mod, name):
+    g = load_golden(name)
+    P = oracle_mod.decompose_scene(golden_surfaces(g), f64=False)
+    boxes = nrt_mod.patch_bounds(P.cp, P.off, P.deg)
+    assert np.array_equal(boxes, oracle_mod.patch_boxes(P))
+    nb, lf, cnt, order, used = nrt_mod.build_bvh_binary(boxes, nrt_mod.BVH_EXACT_SAH)
+    M = g["bvh_box"].shape[0]
+    assert np.array_equal(nb[:M], g["bvh_box"])
+    assert np.array_equal(lf[:M], g["bvh_lf"])
+    assert np.array_equal(cnt[:M], g["bvh_cnt"])
+    assert np.array_equal(order, g["bvh_order"])
+
+
+def _check_bvh_invariants(nb, lf, cnt, order, used, boxes):
+    N = boxes.shape[0]
+    assert sorted(order.tolist()) == list(range(N))
+    seen = np.zeros(N, bool)
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        if cnt[i] > 0:
+            for s in range(lf[i], lf[i] + cnt[i]):
+                seen[s] = True
+                b = boxes[order[s]]
+                assert np.all(nb[i, :3] <= b[:3]) and np.all(nb[i, 3:] >= b[3:])
+        else:
+            for c in (lf[i], lf[i] + 1):
+                assert c < used
+                assert np.all(nb[i, :3] <= nb[c, :3]) and np.all(nb[i, 3:] >= nb[c, 3:])
+                stack.append(c)
+    assert seen.all()
+
+
+def test_binned_bvh_invariants(nrt_mod, oracle_mod):
+    from nrt import scenes
+
+    sc = scenes.surfaces_grid_scene(8, seed=2, width=8, height=8, spp=1)
+    P = oracle_mod.decompose_scene(sc.surfaces, f64=False)
+    boxes = nrt_mod.patch_bounds(P.cp, P.off, P.deg)
+    _check_bvh_invariants(*nrt_mod.build_bvh_binary(boxes, nrt_mod.BVH_BINNED_SAH), boxes)
+    _check_bvh_invariants(*nrt_mod.build_bvh_binary(boxes[:1], nrt_mod.BVH_BINNED_SAH), boxes[:1])
+    # identical boxes cannot be split
+    same = np.repeat(boxes[:1], 5, axis=0)
+    nb, lf, cnt, order, used = nrt_mod.build_bvh_binary(same, nrt_mod.BVH_BINNED_SAH)
+    assert used == 1 and cnt[0] == 5
+
+
+def test_invalid_inputs_report_errors(nrt_mod):
+    from nrt import scenes
+
+    s = scenes.heightfield_scene().surfaces[0]
+    bad = scenes.Surface(s.cp, s.U, s.V, s.n, s.m, 9, s.q)
+    with pytest.raises(nrt_mod.NrtError, match="degree"):
+        nrt_mod.decompose(bad)
+    U = s.U.copy()
+    U[5], U[6] = U[6], U[5] + 0.5
+    with pytest.raises(nrt_mod.NrtError, match="non-decreasing"):
+        nrt_mod.decompose(scenes.Surface(s.cp, U, s.V, s.n, s.m, s.p, s.q))
+    U = s.U.copy()
+    U[s.p] = 0.5 * U[s.p + 1]
+    with pytest.raises(nrt_mod.NrtError, match="clamped"):
+        nrt_mod.decompose(scenes.Surface(s.cp, U, s.V, s.n, s.m, s.p, s.q))
+    assert nrt_mod.lib().nrt_decompose(None, None, None, None, None) == 1
