@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Throughput of the NURBS ray-intersection path on B200 (Mrays/s).
+
+Workload: 64 random NURBS surfaces of degree 2-5 (nets 16x16..32x32, about
+13k Bezier patches), 1920x1080 pixels x 4 jittered samples = 8,294,400 rays
+per step, all seeded and synthetic.  A step is one nrt_intersect over the
+whole batch: closest hit by BVH traversal and rational Newton, FP32 with the
+FP64 final step.  Rays (199 MB) and hits (133 MB) are larger than the 126 MB
+L2, so no flush is needed between steps (the ~7 MB scene stays L2-resident,
+as it would in use).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl nrt|reference]
+
+Under torchrun each rank traces its own batch (different jitter seeds) with no
+collective on the data path (weak scaling); the reported time is the max over
+ranks.  --impl reference times the reference's own CPU code for the path
+(oracle/_ref, compiled from the reference sources) on the host cores.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "rt-nurbs_b200"))
+
+METRIC = "Mrays/s on 1 B200: learned-init wavefront vs plain Newton at equal hit error"
+WORKLOAD = "64 NURBS surfaces deg 2-5, ~13k Bezier patches, 1920x1080x4spp = 8,294,400 rays/step"
+
+
+def f_iter(p, q):
+    """Algorithmic FP32 flops of one Newton evaluation+step on a (p,q) patch:
+    minimal tensor de Casteljau for S, S_u, S_v plus dehomogenisation, residual,
+    Jacobian and 2x2 solve (FMA = 2 flops, vec4 lerp = 12, vec4 difference = 8)."""
+    return 12 * ((p + 1) * q * (q + 1) // 2 + p * (p + 1)) + 8 * (p + 2) + 80
+
+
+def algorithmic_flops(c):
+    fl = 12 * c["box_tests"] + 40 * c["rays"]
+    for (p, q), n in c["evals_by_degree"].items():
+        fl += n * f_iter(p, q)
+    for (p, q), n in c["hull_tests_by_degree"].items():
+        fl += n * 16 * (p + 1) * (q + 1)
+    return fl
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) > 8 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def sgemm_peak_tflops(torch):
+    """FP32 (no TF32) cuBLAS GEMM throughput on this GPU: the measured FP32-pipe denominator."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda")
+    b = torch.randn(n, n, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def ncu_traffic(kernel_tag):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(path)).get(kernel_tag)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(scene_def, rays_np, seconds=10.0, iters=8, eps=1e-6, port=False):
+    """Mrays/s of the reference's own FP32 path on the host cores (oracle/_ref,
+    OpenMP over rays) on a bounded sample of the workload's rays.  The BVH is
+    this project's binned-SAH tree exported in the reference's node layout (the
+    reference's own O(N^2) builder takes minutes at this size; the closest hit
+    does not depend on the tree)."""
+    import nrt
+    import oracle
+
+    P = oracle.decompose_scene(scene_def.surfaces, f64=False)
+    boxes = nrt.patch_bounds(P.cp, P.off, P.deg)
+    nb, lf, cnt, order, used = nrt.build_bvh_binary(boxes, nrt.BVH_BINNED_SAH)
+    bvh = oracle.BinaryBVH(nb, lf, cnt, order, used)
+    use_ref = oracle.ref_available(iters) and not port
+    Pb = P.subset(order)
+    n = rays_np.n
+
+    def run(idx):
+        r = rays_np.take(idx)
+        t0 = time.perf_counter()
+        if use_ref:
+            oracle.ref_intersect(Pb, bvh, r, bilinear_init=False, eps=eps, iters=iters)
+        else:
+            oracle.intersect(P, bvh, r, init_mode=0, max_iter=iters, eps=eps)
+        return time.perf_counter() - t0, r.n
+
+    # calibrate on a small strided sample, then size the sample to ~`seconds`
+    dt, m = run(np.arange(0, n, max(1, n // 20000)))
+    rate = m / max(dt, 1e-9)
+    stride = max(1, int(n / max(1.0, rate * seconds)))
+    idx = np.arange(0, n, stride)
+    return {"run": run, "idx": idx, "kind": "reference" if use_ref else "port",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+            "sample": f"every {stride}th ray of the workload ({idx.size} rays), plain settings "
+                      f"(midpoint init, {iters} evaluations, eps {eps:g})"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from nrt import scenes
+    import oracle
+
+    sc = scenes.mixed_degree_scene(1)
+    rays = oracle.camera_rays(sc.camera)
+    cb = cpu_reference_rate(sc, rays, seconds=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cb["run"](cb["idx"])
+    ts = []
+    for _ in range(args.steps):
+        dt, m = cb["run"](cb["idx"])
+        ts.append(dt)
+    total = sum(ts)
+    value = args.steps * cb["idx"].size / total / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "sample_rays_per_step": int(cb["idx"].size)},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cb["cores"], "kind": cb["kind"],
+                             "sample": cb["sample"]},
+            "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def nrt_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import nrt
+    from nrt import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sc = scenes.mixed_degree_scene(1)
+    sc.camera.seed = 1 + rank  # each rank its own samples
+    t0 = time.perf_counter()
+    scene = nrt.Scene(sc.surfaces)
+    build_s = time.perf_counter() - t0
+    rays = nrt.camera_rays(sc.camera)
+    n = rays[0].numel()
+    stream = torch.cuda.current_stream()
+    best = nrt.default_opts(hull_cull=1, fp64_final=1, cond_fp64=1e4)
+    plain = nrt.default_opts()
+    out = {"patch": torch.empty(n, dtype=torch.int32, device="cuda"),
+           "t": torch.empty(n, dtype=torch.float32, device="cuda"),
+           "u": torch.empty(n, dtype=torch.float32, device="cuda"),
+           "v": torch.empty(n, dtype=torch.float32, device="cuda")}
+
+    def step(opts):
+        scene.intersect(rays, opts, out=out, stream=stream)
+
+    def timed(opts, k, w):
+        for _ in range(w):
+            step(opts)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(k):
+            step(opts)
+        e.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = s.elapsed_time(e)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    if args.profile:
+        # only the path's kernels, for ncu: warmup + steps launches of the timed configuration
+        for _ in range(args.warmup + args.steps):
+            step(best)
+        torch.cuda.synchronize()
+        scene.close()
+        return
+    peaks = measured_peaks()
+    sgemm = sgemm_peak_tflops(torch)
+    # counted run (separate from timing) for algorithmic flops and iteration statistics
+    scene.enable_counters(True)
+    step(best)
+    cnt = scene.counters()
+    scene.enable_counters(False)
+    flops = algorithmic_flops(cnt)
+
+    with ClockSampler(local) as clk:
+        ms_total = timed(best, args.steps, args.warmup)
+    ms_step = ms_total / args.steps
+    value = world * n * args.steps / (ms_total * 1e-3) / 1e6
+
+    ms_plain = timed(plain, max(1, args.steps // 2), 1) / max(1, args.steps // 2)
+
+    # end to end through the public API: pinned host rays -> device -> intersect -> hits back to host
+    host_rays = [a.cpu().pin_memory() for a in rays]
+    dev_rays = [torch.empty_like(a) for a in rays]
+    host_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in out.items()}
+
+    def e2e_step():
+        for h, d in zip(host_rays, dev_rays):
+            d.copy_(h, non_blocking=True)
+        scene.intersect(dev_rays, best, out=out, stream=stream)
+        for k in out:
+            host_out[k].copy_(out[k], non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = s.elapsed_time(e)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n * args.steps / (e2e_ms * 1e-3) / 1e6
+
+    line = None
+    if rank == 0:
+        achieved = flops / (ms_step * 1e-3) / 1e12
+        roof = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(sgemm, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / sgemm, 4), "traffic": ncu_traffic("k_intersect_pixel"),
+                "peak_source": "measured in this run: cuBLAS FP32 SGEMM 8192^3, TF32 off (burst)",
+                "flops_per_launch": int(flops),
+                "hbm": {"achieved_gbs": round(40.0 * n / (ms_step * 1e-3) / 1e9, 2),
+                        "peak_gbs": peaks.get("hbm_gbs"), "algorithmic_bytes_per_ray": 40}}
+        cpu = None
+        if not args.no_cpu_baseline:
+            import oracle
+
+            rays_np = oracle.Rays(*[a.cpu().numpy() for a in rays])
+            cb = cpu_reference_rate(sc, rays_np, seconds=10.0)
+            dt, m = cb["run"](cb["idx"])
+            cpu = {"value": round(m / dt / 1e6, 4), "unit": "Mrays/s", "cores": cb["cores"], "kind": cb["kind"],
+                   "sample": cb["sample"]}
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and rays)",
+                "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": n, "patches": scene.info()["n_patches"],
+                           "schedule": "pixel", "opts": {k: (round(v, 9) if isinstance(v, float) else v)
+                                                          for k, v in best.as_dict().items()},
+                           "l2": "inputs (199 MB rays) and outputs (133 MB) exceed the 126 MB L2; no flush",
+                           "scene_build_s": round(build_s, 3)},
+                "plain_pixel": {"value": round(world * n / (ms_plain * 1e-3) / 1e6, 3), "ms_per_step": round(ms_plain, 3),
+                                "opts": "midpoint init, 8 evaluations, eps 1e-6, no cull, no FP64"},
+                "iterations": {"newton_evals_per_ray": round(cnt["newton_evals"] / cnt["rays"], 3),
+                               "newton_solves_per_ray": round(cnt["newton_solves"] / cnt["rays"], 3),
+                               "culled_per_ray": round(cnt["patch_culled"] / cnt["rays"], 3),
+                               "box_tests_per_ray": round(cnt["box_tests"] / cnt["rays"], 3),
+                               "fp64_solve_frac": round(cnt["fp64_solves"] / max(1, cnt["newton_evals"]), 5),
+                               "hit_rate": round(cnt["hits"] / cnt["rays"], 4)},
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 24 * n,
+                        "d2h_bytes_per_step": 16 * n},
+                "gpu_launches": args.steps, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nrt", choices=["nrt", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="only launch the timed kernels (for ncu)")
+    args = ap.parse_args()
+    if args.warmup < 3 and not args.profile:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        nrt_arm(args)
+
+
+if __name__ == "__main__":
+    main()
