@@ -92,6 +92,8 @@ typedef struct {
     int builder;        /* NRT_BVH_BINNED_SAH (default) or NRT_BVH_EXACT_SAH */
     int max_leaf;       /* patches per BVH leaf (1..8, default 1) */
     int device;         /* CUDA device ordinal */
+    int64_t wavefront_chunk; /* rays per wavefront pass (0 = 2^23); bounds its scratch,
+                                about 530 bytes per ray, allocated on first use */
 } nrt_build_opts;
 
 int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nrt_build_opts* opts,
@@ -180,6 +182,8 @@ typedef struct {
         fp64_final_steps, hits, errors;
     uint64_t evals_by_degree[64];      /* Newton evaluations per (p,q), index p*8+q */
     uint64_t hull_tests_by_degree[64]; /* hull tests per (p,q) */
+    uint64_t kernel_launches;          /* kernels launched by the last nrt_intersect (host count) */
+    uint64_t rounds;                   /* wavefront rounds of the last nrt_intersect */
 } nrt_counters;
 int nrt_enable_counters(nrt_scene* scene, int enable);
 int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream);

@@ -13,6 +13,7 @@
 
 #include "kernels.h"
 #include "nrt_internal.h"
+#include "wavefront.h"
 
 // ---------------------------------------------------------------------------
 namespace nrt {
@@ -92,7 +93,16 @@ struct nrt_scene {
     int counters_on = 0;
     dev::Scene view{};
     nrt_scene_info info{};
+    dev::WfPlan plan{};
+    void* wf_ws = nullptr;       // wavefront scratch, grown on demand
+    size_t wf_bytes = 0;
+    long long wf_rays = 0;       // rays the scratch was carved for
+    long long wf_chunk = 0;      // rays per wavefront pass
+    int32_t* host_count = nullptr;  // pinned word for the per-round active count
+    long long last_launches = 0, last_rounds = 0;  // of the last nrt_intersect
 };
+
+
 
 namespace {
 
@@ -101,8 +111,9 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     *out = nullptr;
     const int N = ps.count();
     if (N <= 0) return fail(NRT_ERR_INVALID, "scene has no patches");
-    nrt_build_opts o{NRT_BVH_BINNED_SAH, 1, 0};
+    nrt_build_opts o{NRT_BVH_BINNED_SAH, 1, 0, 0};
     if (opts) o = *opts;
+    if (o.wavefront_chunk < 0) return fail(NRT_ERR_INVALID, "negative wavefront_chunk");
     if (o.max_leaf < 1 || o.max_leaf > 8) return fail(NRT_ERR_INVALID, "max_leaf must be in 1..8");
     if (N >= (1 << 27)) return fail(NRT_ERR_INVALID, "too many patches (%d)", N);
     for (int k = 0; k < N; ++k) {
@@ -180,11 +191,30 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     const size_t sz_nodes = align(wide.size() * sizeof(Node4)), sz_hdr = align(N * sizeof(int4)),
                  sz_cen = align(N * sizeof(double4)), sz_cp = align(blocks.size() * sizeof(float)),
                  sz_cor = align(corners.size() * sizeof(float4)), sz_del = align(N * sizeof(float)),
-                 sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long));
-    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr;
+                 sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long)),
+                 sz_rank = align(N * sizeof(int32_t));
+    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank;
+    // wavefront plan: patches ranked by (p, q, slot); one class per degree pair present
+    std::vector<int32_t> by_rank(N), rank_of(N);
+    for (int s2 = 0; s2 < N; ++s2) by_rank[s2] = s2;
+    std::stable_sort(by_rank.begin(), by_rank.end(), [&](int a, int b) { return (hdr[a].y & 0xff) < (hdr[b].y & 0xff); });
+    dev::WfPlan plan{};
+    plan.n_slots = N;
+    for (int rk = 0; rk < N; ++rk) {
+        rank_of[by_rank[rk]] = rk;
+        const int pq = hdr[by_rank[rk]].y & 0xff;
+        if (plan.n_classes == 0 || plan.class_pq[plan.n_classes - 1] != pq) {
+            plan.class_pq[plan.n_classes] = pq;
+            plan.class_rank[plan.n_classes] = rk;
+            plan.class_grid[plan.n_classes] = 148 * 4;
+            ++plan.n_classes;
+        }
+    }
+    plan.class_rank[plan.n_classes] = N;
     nrt_scene* sc = new (std::nothrow) nrt_scene();
     if (!sc) return fail(NRT_ERR_NOMEM, "host allocation failed");
     sc->device = o.device;
+    sc->wf_chunk = o.wavefront_chunk > 0 ? o.wavefront_chunk : (1LL << 23);
     int prev = 0;
     cudaGetDevice(&prev);
     cudaError_t e = cudaSetDevice(o.device);
@@ -207,6 +237,9 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     sc->view.delta = static_cast<const float*>(put(delta.data(), N * sizeof(float), sz_del));
     sc->counters = reinterpret_cast<unsigned long long*>(base + at);
     if (e == cudaSuccess) e = cudaMemset(sc->counters, 0, sz_ctr);
+    at += sz_ctr;
+    plan.rank_of = static_cast<const int32_t*>(put(rank_of.data(), N * sizeof(int32_t), sz_rank));
+    sc->plan = plan;
     cudaSetDevice(prev);
     if (e != cudaSuccess) {
         cudaFree(sc->arena);
@@ -365,6 +398,11 @@ int nrt_scene_destroy(nrt_scene* scene) {
     cudaGetDevice(&prev);
     cudaSetDevice(scene->device);
     cudaError_t e = cudaFree(scene->arena);
+    if (scene->wf_ws) {
+        const cudaError_t e2 = cudaFree(scene->wf_ws);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (scene->host_count) cudaFreeHost(scene->host_count);
     cudaSetDevice(prev);
     delete scene;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFree(scene)");
@@ -421,7 +459,10 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
         if (o.init_mode == NRT_INIT_LEARNED) return fail(NRT_ERR_UNSUPPORTED, "learned init needs a trained model");
         return fail(NRT_ERR_INVALID, "unknown init mode %d", o.init_mode);
     }
-    if (o.schedule != NRT_SCHED_PIXEL) return fail(NRT_ERR_UNSUPPORTED, "schedule %d not available", o.schedule);
+    if (o.schedule != NRT_SCHED_PIXEL && o.schedule != NRT_SCHED_WAVEFRONT)
+        return fail(NRT_ERR_INVALID, "unknown schedule %d", o.schedule);
+    if (o.schedule == NRT_SCHED_WAVEFRONT && o.flat_threshold > 0.f)
+        return fail(NRT_ERR_UNSUPPORTED, "flat-skip runs on the per-pixel schedule only");
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != scene->device) NRT_CUDA(cudaSetDevice(scene->device), "cudaSetDevice");
@@ -433,7 +474,49 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
                  "counter reset");
     dev::Rays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz};
     dev::Hits h{hits->patch, hits->t, hits->u, hits->v, hits->iters, hits->tests, hits->geom};
-    cudaError_t e = dev::launch_intersect_pixel(scene->view, r, (long long)n, d, h, scene->counters, st);
+    cudaError_t e = cudaSuccess;
+    scene->last_launches = 0;
+    scene->last_rounds = 0;
+    if (o.schedule == NRT_SCHED_PIXEL) {
+        e = dev::launch_intersect_pixel(scene->view, r, (long long)n, d, h, scene->counters, st);
+        scene->last_launches = 1;
+    } else {
+        const long long chunk = std::min<long long>(n, scene->wf_chunk);
+        if (scene->wf_rays < chunk) {
+            // (re)allocate scratch for `chunk` rays; cudaFree synchronises the device
+            if (scene->wf_ws) cudaFree(scene->wf_ws);
+            scene->wf_ws = nullptr;
+            scene->wf_rays = 0;
+            const size_t bytes = dev::wavefront_scratch_bytes(chunk, scene->plan.n_slots);
+            e = cudaMalloc(&scene->wf_ws, bytes);
+            if (e != cudaSuccess) {
+                scene->wf_ws = nullptr;
+                if (prev != scene->device) cudaSetDevice(prev);
+                return cuda_fail(e, "cudaMalloc(wavefront scratch)");
+            }
+            scene->wf_bytes = bytes;
+            scene->wf_rays = chunk;
+        }
+        if (!scene->host_count) {
+            e = cudaMallocHost(&scene->host_count, sizeof(int32_t));
+            if (e != cudaSuccess) {
+                scene->host_count = nullptr;
+                if (prev != scene->device) cudaSetDevice(prev);
+                return cuda_fail(e, "cudaMallocHost(count)");
+            }
+        }
+        const dev::WfBuffers wb = dev::wavefront_carve(scene->wf_ws, scene->wf_rays, scene->plan.n_slots);
+        for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
+            const long long m = std::min(chunk, (long long)n - at);
+            dev::Rays rc{r.ox + at, r.oy + at, r.oz + at, r.dx + at, r.dy + at, r.dz + at};
+            dev::Hits hc{h.patch + at, h.t + at, h.u + at, h.v + at, h.iters ? h.iters + at : nullptr,
+                         h.tests ? h.tests + at : nullptr, h.geom ? h.geom + 9 * at : nullptr};
+            dev::Opts dc = d;
+            dc.seed_offset = d.seed_offset + (uint32_t)at;  // seeds follow the global ray index
+            e = dev::launch_wavefront(scene->view, scene->plan, rc, m, dc, hc, wb, scene->host_count,
+                                      scene->counters, st, &scene->last_launches, &scene->last_rounds);
+        }
+    }
     if (prev != scene->device) cudaSetDevice(prev);
     if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
     return NRT_OK;
@@ -461,6 +544,8 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
     out->fp64_final_steps = h[dev::kFp64Final];
     out->hits = h[dev::kHits];
     out->errors = h[dev::kErrors];
+    out->kernel_launches = (uint64_t)scene->last_launches;
+    out->rounds = (uint64_t)scene->last_rounds;
     for (int k = 0; k < 64; ++k) {
         out->evals_by_degree[k] = h[dev::kEvalsByDegree + k];
         out->hull_tests_by_degree[k] = h[dev::kHullByDegree + k];

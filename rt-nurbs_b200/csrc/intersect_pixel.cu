@@ -8,6 +8,7 @@
 
 #include "device_scene.cuh"
 #include "kernels.h"
+#include "wavefront.h"
 
 namespace nrt {
 namespace dev {
@@ -90,10 +91,8 @@ __device__ __noinline__ void test_patch_any(const Scene& sc, int slot, const Ray
     }
 }
 
-__global__ void __launch_bounds__(128) k_intersect_pixel(Scene sc, Rays rays, long long n, Opts op, Hits out,
-                                                         unsigned long long* ctr) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ void trace_pixel(const Scene& sc, const Rays& rays, long long i, const Opts& op,
+                                            const Hits& out, unsigned long long* ctr) {
     RayFrame r;
     r.ox = rays.ox[i]; r.oy = rays.oy[i]; r.oz = rays.oz[i];
     r.dx = rays.dx[i]; r.dy = rays.dy[i]; r.dz = rays.dz[i];
@@ -199,12 +198,37 @@ __global__ void __launch_bounds__(128) k_intersect_pixel(Scene sc, Rays rays, lo
     }
 }
 
+__global__ void __launch_bounds__(128) k_intersect_pixel(Scene sc, Rays rays, long long n, Opts op, Hits out,
+                                                         unsigned long long* ctr) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) trace_pixel(sc, rays, i, op, out, ctr);
+}
+
+// Same, for the ray indices list[0 .. *count) (count known only on the device).
+__global__ void __launch_bounds__(128) k_intersect_pixel_list(Scene sc, Rays rays, const int32_t* list,
+                                                              const int32_t* count, Opts op, Hits out,
+                                                              unsigned long long* ctr) {
+    const int m = *count;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        trace_pixel(sc, rays, list[k], op, out, ctr);
+}
+
 cudaError_t launch_intersect_pixel(const Scene& sc, const Rays& rays, long long n, const Opts& op, const Hits& out,
                                    unsigned long long* ctr, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     const int threads = 128;
     const long long blocks = (n + threads - 1) / threads;
     k_intersect_pixel<<<(unsigned)blocks, threads, 0, stream>>>(sc, rays, n, op, out, ctr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const int32_t* list,
+                                        const int32_t* list_count, long long max_n, const Opts& op, const Hits& out,
+                                        unsigned long long* ctr, cudaStream_t stream) {
+    if (max_n <= 0) return cudaSuccess;
+    long long blocks = (max_n + 127) / 128;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_intersect_pixel_list<<<(unsigned)blocks, 128, 0, stream>>>(sc, rays, list, list_count, op, out, ctr);
     return cudaGetLastError();
 }
 

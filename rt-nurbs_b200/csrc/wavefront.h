@@ -1,0 +1,63 @@
+// wavefront.h -- buffers and plan of the batched (wavefront) schedule.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_scene.cuh"
+
+namespace nrt {
+namespace dev {
+
+constexpr int kEmitMax = 32;   // candidates one ray may emit in one round (K <= 24, plus one leaf)
+constexpr unsigned long long kNoHit = ~0ull;
+
+// Candidates per ray in round r: 1, 2, 4, 8, 16, then 24.
+__host__ __device__ constexpr int round_quota(int r) { return r >= 5 ? 24 : (1 << r); }
+
+// Scratch of one wavefront launch over n rays (device pointers).
+struct WfBuffers {
+    int32_t* stack_ref;            // kStack * n, entry k of ray i at [k * n + i]
+    float* stack_t;                // kStack * n
+    int32_t* stack_sp;             // n
+    unsigned long long* best_key;  // n: (t bits << 32) | slot of the nearest hit so far
+    int32_t* active[2];            // n each: ray indices still traversing (ping-pong)
+    int32_t* counts;               // 4 ints: active count of the two lists, items of the round
+    int32_t* emit_slot;            // n * kEmitMax: candidates emitted this round, by active position
+    int32_t* emit_cnt;             // n
+    int2* items;                   // n * kEmitMax: (ray, slot) work items of a round, in rank order
+    int32_t* hist;                 // n_slots + 1
+    int32_t* cursor;               // n_slots + 1
+    int32_t* offsets;              // n_slots + 1
+};
+
+// Per-scene schedule data: patch ranks in (p, q, slot) order and the degree
+// classes present.
+struct WfPlan {
+    const int32_t* rank_of;   // device: slot -> rank
+    int n_slots;
+    int n_classes;
+    int class_pq[64];         // p | q << 4
+    int class_rank[65];       // first rank of each class; [n_classes] = n_slots
+    unsigned class_grid[64];  // blocks of 256 threads for the class's Newton kernel
+};
+
+// Bytes of scratch for n rays and a scene of n_slots patches.
+size_t wavefront_scratch_bytes(long long n, int n_slots);
+// Carve WfBuffers out of one block of at least wavefront_scratch_bytes(n, n_slots).
+WfBuffers wavefront_carve(void* base, long long n, int n_slots);
+
+// Runs the rounds; synchronises `stream` once per round to read the number of
+// rays still traversing into host_count (pinned host memory).
+cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
+                             const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
+                             cudaStream_t stream, long long* launches, long long* rounds);
+
+// Per-pixel kernel over a device list of ray indices (count read on the device).
+cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const int32_t* list,
+                                        const int32_t* list_count, long long max_n, const Opts& op, const Hits& out,
+                                        unsigned long long* ctr, cudaStream_t stream);
+
+}  // namespace dev
+}  // namespace nrt

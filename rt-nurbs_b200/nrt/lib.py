@@ -26,7 +26,7 @@ class NurbsSurface(C.Structure):
 
 
 class BuildOpts(C.Structure):
-    _fields_ = [("builder", C.c_int), ("max_leaf", C.c_int), ("device", C.c_int)]
+    _fields_ = [("builder", C.c_int), ("max_leaf", C.c_int), ("device", C.c_int), ("wavefront_chunk", C.c_int64)]
 
 
 class SceneInfo(C.Structure):
@@ -64,12 +64,15 @@ _COUNTER_NAMES = ("rays", "box_tests", "patch_candidates", "patch_culled", "newt
 
 class Counters(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in _COUNTER_NAMES] + [("evals_by_degree", C.c_uint64 * 64),
-                                                            ("hull_tests_by_degree", C.c_uint64 * 64)]
+                                                            ("hull_tests_by_degree", C.c_uint64 * 64),
+                                                            ("kernel_launches", C.c_uint64), ("rounds", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: int(getattr(self, k)) for k in _COUNTER_NAMES}
         d["evals_by_degree"] = {(k // 8, k % 8): int(v) for k, v in enumerate(self.evals_by_degree) if v}
         d["hull_tests_by_degree"] = {(k // 8, k % 8): int(v) for k, v in enumerate(self.hull_tests_by_degree) if v}
+        d["kernel_launches"] = int(self.kernel_launches)
+        d["rounds"] = int(self.rounds)
         return d
 
 
@@ -194,10 +197,10 @@ def _stream_ptr(stream):
 class Scene:
     """A device scene (decomposition + BVH + upload), nrt_scene_create."""
 
-    def __init__(self, surfaces=None, patches=None, builder=BVH_BINNED_SAH, max_leaf=1, device=0):
+    def __init__(self, surfaces=None, patches=None, builder=BVH_BINNED_SAH, max_leaf=1, device=0, wavefront_chunk=0):
         L = lib()
         self._h = C.c_void_p()
-        opts = BuildOpts(builder, max_leaf, device)
+        opts = BuildOpts(builder, max_leaf, device, wavefront_chunk)
         if surfaces is not None:
             arr = (NurbsSurface * len(surfaces))()
             keep = []

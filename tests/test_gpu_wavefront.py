@@ -1,0 +1,107 @@
+"""GPU parity of the wavefront schedule (through the C ABI).
+
+Tolerances:
+  * against the per-pixel schedule with the same options: identical hit/miss
+    on >= 99.99% of rays, the same patch on >= 99.9% of rays both hit (the two
+    may pick different patches only on exact ties), identical (bit-equal) t, u,
+    v where they pick the same patch.
+  * against the FP64 oracle (same method): hit/miss agreement >= 99.99%,
+    relative t error <= 1e-4 and (u,v) error <= 1e-3 on same-patch hits.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_rays, golden_surfaces, load_golden
+from parity import compare, gpu_rays, to_numpy
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nrt_gpu():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import nrt
+
+    nrt.lib()
+    return nrt
+
+
+def same_as_pixel(nrt_gpu, scene, rays, base):
+    a = to_numpy(scene.intersect(rays, base.replace(schedule=nrt_gpu.SCHED_PIXEL)))
+    b = to_numpy(scene.intersect(rays, base.replace(schedule=nrt_gpu.SCHED_WAVEFRONT)))
+    hit_a, hit_b = a["patch"] >= 0, b["patch"] >= 0
+    assert (hit_a == hit_b).mean() >= 0.9999
+    both = hit_a & hit_b
+    same = both & (a["patch"] == b["patch"])
+    assert same.sum() >= 0.999 * both.sum()
+    for k in ("t", "u", "v", "iters"):
+        assert np.array_equal(a[k][same], b[k][same]), k
+    return a, b
+
+
+@pytest.mark.parametrize("name", ["heightfield", "torus", "sphere", "mixed4"])
+def test_wavefront_matches_pixel_on_fixtures(nrt_gpu, name):
+    g = load_golden(name)
+    scene = nrt_gpu.Scene(golden_surfaces(g))
+    rays = gpu_rays(golden_rays(g))
+    for base in [nrt_gpu.default_opts(), nrt_gpu.default_opts(hull_cull=1, fp64_final=1, cond_fp64=1e4),
+                 nrt_gpu.reference_opts(), nrt_gpu.reference_opts(hull_cull=1)]:
+        same_as_pixel(nrt_gpu, scene, rays, base)
+
+
+def test_wavefront_many_surfaces_vs_fp64(nrt_gpu, oracle_mod):
+    """16 mixed-degree surfaces, 320x180x2 jittered rays, against the FP64 oracle."""
+    from nrt import scenes
+
+    sc = scenes.surfaces_grid_scene(16, seed=5, width=320, height=180, spp=2)
+    scene = nrt_gpu.Scene(sc.surfaces)
+    rays = nrt_gpu.camera_rays(sc.camera)
+    opts = nrt_gpu.default_opts(hull_cull=1, fp64_final=1, cond_fp64=1e4, schedule=nrt_gpu.SCHED_WAVEFRONT)
+    out = to_numpy(scene.intersect(rays, opts))
+    P = oracle_mod.decompose_scene(sc.surfaces, f64=False)
+    P.cp64 = P.cp.astype(np.float64)
+    nb, lf, cnt, order, used = nrt_gpu.build_bvh_binary(nrt_gpu.patch_bounds(P.cp, P.off, P.deg),
+                                                        nrt_gpu.BVH_BINNED_SAH)
+    r_np = oracle_mod.Rays(*[a.cpu().numpy() for a in rays])
+    ref = oracle_mod.intersect(P, oracle_mod.BinaryBVH(nb, lf, cnt, order, used), r_np, 0, 8, 1e-6, f64=True)
+    st = compare(out, ref.patch, ref.t, ref.u, ref.v)
+    assert st["hit_rate"] > 0.3, st
+    assert st["agree"] >= 0.9999, st
+    assert st["t_rel_max"] <= 1e-4, st
+    assert st["uv_abs_p999"] <= 1e-3, st
+    same_as_pixel(nrt_gpu, scene, rays, opts)
+
+
+def test_wavefront_chunks_and_overflow(nrt_gpu):
+    """Small chunks (many passes) and rays with more candidates than a list
+    holds (per-pixel fallback) give the per-pixel results."""
+    import torch
+
+    from nrt import scenes
+
+    # 48 stacked parallel bilinear sheets: a ray along z crosses all of them
+    cp, off, deg = [], [], []
+    for k in range(48):
+        z = 0.1 * k
+        for (x, y) in [(0, 0), (0, 1), (1, 0), (1, 1)]:
+            cp.append([x, y, z, 1.0])
+        off.append(4 * k)
+        deg.append([1, 1])
+    cp = np.array(cp, np.float32)
+    scene = nrt_gpu.Scene(patches=(cp, np.array(off, np.int32), np.array(deg, np.int32)), wavefront_chunk=100)
+    n = 1000
+    rng = np.random.default_rng(0)
+    o = np.stack([rng.uniform(0.05, 0.95, n), rng.uniform(0.05, 0.95, n), np.full(n, -1.0)], 1).astype(np.float32)
+    d = np.tile(np.array([[0.0, 0.0, 1.0]], np.float32), (n, 1))
+    d[::2] = np.array([0.05, 0.02, 1.0]) / np.linalg.norm([0.05, 0.02, 1.0])
+    rays = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (o[:, 0], o[:, 1], o[:, 2], d[:, 0], d[:, 1], d[:, 2])]
+    a, b = same_as_pixel(nrt_gpu, scene, rays, nrt_gpu.default_opts(hull_cull=1))
+    near = a["patch"] == 0  # the nearest sheet, at z = 0
+    assert near.mean() > 0.9
+    np.testing.assert_allclose(a["t"][near], 1.0 / d[near, 2], rtol=1e-6)
+    sc = scenes.heightfield_scene(0, 64, 48)
+    scene = nrt_gpu.Scene(sc.surfaces, wavefront_chunk=777)
+    same_as_pixel(nrt_gpu, scene, nrt_gpu.camera_rays(sc.camera), nrt_gpu.default_opts(hull_cull=1, fp64_final=1))
