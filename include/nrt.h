@@ -176,6 +176,22 @@ void nrt_reference_opts(nrt_intersect_opts* opts);
 int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
                   const nrt_hits* hits, void* stream);
 
+/* Intersection without any allocation, for callers that cannot allocate GPU
+ * memory while they run: real-time or embedded loops with a fixed memory
+ * budget, or code under a memory pool that owns the device.  No reference
+ * counterpart: the reference has no scratch-free entry point (its kernel uses
+ * no scratch at all, src/gpu/intersect.cu:20-194).
+ * It runs the wavefront schedule (opts->schedule is ignored) with its scratch
+ * in a fixed 64 MiB array inside libnrt.so, which every GPU that loads the
+ * library holds until the process exits; rays go through in passes that fit
+ * that array.  Scenes too large for it (about 5 million patches and more) are
+ * rejected with NRT_ERR_INVALID.  The first call on a device looks the array
+ * up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array, so calls whose work overlaps on the GPU race:
+ * serialise them on one stream.  Synchronises `stream` once per round. */
+int nrt_intersect_noalloc(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                          const nrt_hits* hits, void* stream);
+
 /* Counters of the last nrt_intersect on this scene (synchronises the stream). */
 typedef struct {
     uint64_t rays, box_tests, patch_candidates, patch_culled, newton_solves, newton_evals, fp64_solves,

@@ -597,3 +597,36 @@ int nrt_generate_camera_rays(const nrt_camera* cam, const nrt_rays_out* out, voi
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Views for nrt_intersect_noalloc (noalloc.cu): validates the arguments as
+// nrt_intersect does and hands out the scene's device views; allocates nothing.
+namespace nrt {
+
+int noalloc_views(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                  const nrt_hits* hits, NoallocViews* v) {
+    if (!scene || !rays || !opts || !hits || !v) return fail(NRT_ERR_INVALID, "null argument");
+    if (n < 0) return fail(NRT_ERR_INVALID, "negative ray count");
+    if (n > 0 && (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz))
+        return fail(NRT_ERR_INVALID, "null ray array");
+    if (n > 0 && (!hits->patch || !hits->t || !hits->u || !hits->v)) return fail(NRT_ERR_INVALID, "null hit array");
+    const nrt_intersect_opts& o = *opts;
+    if (o.max_iter < 1 || o.max_iter > 256) return fail(NRT_ERR_INVALID, "max_iter %d outside 1..256", o.max_iter);
+    if (!(o.eps > 0.f)) return fail(NRT_ERR_INVALID, "eps must be positive");
+    if (o.init_mode != NRT_INIT_MIDPOINT && o.init_mode != NRT_INIT_BILINEAR)
+        return fail(NRT_ERR_UNSUPPORTED, "init mode %d not available without allocation", o.init_mode);
+    if (o.flat_threshold > 0.f) return fail(NRT_ERR_UNSUPPORTED, "flat-skip runs on the per-pixel schedule only");
+    v->scene = scene->view;
+    v->plan = scene->plan;
+    v->counters = scene->counters;
+    v->device = scene->device;
+    to_dev_opts(o, v->opts, scene->counters_on);
+    return NRT_OK;
+}
+
+void noalloc_record(nrt_scene* scene, long long launches, long long rounds) {
+    scene->last_launches = launches;
+    scene->last_rounds = rounds;
+}
+
+}  // namespace nrt

@@ -58,4 +58,10 @@ static_assert(sizeof(Node4) == 128, "Node4 must be 128 bytes");
 // Collapse a binary BVH into 4-wide nodes; leaf slots keep the binary order.
 void collapse_to_wide(const BinaryBVH& bin, std::vector<Node4>& out, int& depth);
 
+// Scene views for nrt_intersect_noalloc (defined in engine.cu, used by noalloc.cu).
+struct NoallocViews;
+int noalloc_views(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                  const nrt_hits* hits, NoallocViews* v);
+void noalloc_record(nrt_scene* scene, long long launches, long long rounds);
+
 }  // namespace nrt

@@ -60,4 +60,13 @@ cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const
                                         unsigned long long* ctr, cudaStream_t stream);
 
 }  // namespace dev
+
+struct NoallocViews {
+    dev::Scene scene;
+    dev::WfPlan plan;
+    dev::Opts opts;
+    unsigned long long* counters;
+    int device;
+};
+
 }  // namespace nrt

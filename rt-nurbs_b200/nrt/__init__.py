@@ -5,6 +5,7 @@ buffers are torch CUDA tensors whose pointers are handed to the C ABI, and
 every compute call goes to the CUDA kernels in libnrt.so.  There is no CPU
 fallback: if the library or a GPU is missing, calls raise.
 """
+from . import lib as lib_module  # noqa: F401
 from .lib import (  # noqa: F401
     BuildOpts,
     Camera,
