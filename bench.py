@@ -229,7 +229,7 @@ def nrt_arm(args):
     rays = nrt.camera_rays(sc.camera)
     n = rays[0].numel()
     stream = torch.cuda.current_stream()
-    best = nrt.default_opts(fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT)
+    best = nrt.default_opts(hull_cull=2, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT)
     plain = nrt.default_opts()
     out = {"patch": torch.empty(n, dtype=torch.int32, device="cuda"),
            "t": torch.empty(n, dtype=torch.float32, device="cuda"),

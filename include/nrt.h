@@ -161,6 +161,8 @@ typedef struct {
     int seed_offset;      /* added to the ray index to seed the singular-Jacobian pull */
     float flat_threshold; /* flat-skip in pixels (src/gpu/intersect.cu:104-123); 0 = off */
     float cam_k;          /* 0.5*H/tan(vfov/2), only used by flat-skip */
+    int learned_iters;    /* NRT_INIT_LEARNED: evaluations from the network's guess before
+                             falling back to plain Newton from (0.5,0.5); 0 = max_iter */
 } nrt_intersect_opts;
 
 /* Fill opts with the plain settings: midpoint init, 8 evaluations, eps 1e-6,
@@ -196,6 +198,8 @@ int nrt_intersect_noalloc(nrt_scene* scene, const nrt_rays* rays, int64_t n, con
 typedef struct {
     uint64_t rays, box_tests, patch_candidates, patch_culled, newton_solves, newton_evals, fp64_solves,
         fp64_final_steps, hits, errors;
+    uint64_t learned_solves;   /* solves started from the network's guess */
+    uint64_t learned_fallbacks;/* of those, how many did not converge and fell back to plain Newton */
     uint64_t evals_by_degree[64];      /* Newton evaluations per (p,q), index p*8+q */
     uint64_t hull_tests_by_degree[64]; /* hull tests per (p,q) */
     uint64_t kernel_launches;          /* kernels launched by the last nrt_intersect (host count) */
@@ -217,6 +221,47 @@ typedef struct {
     uint32_t seed;
 } nrt_camera;
 int nrt_generate_camera_rays(const nrt_camera* cam, const nrt_rays_out* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned initial guess (no reference counterpart: the reference starts every
+ * solve from its bilinear guess, src/gpu/intersect.cu:102).  A 12-64-64-2
+ * MLP with SiLU maps (ray, patch) features to a starting (u, v); BF16 tensor
+ * cores, FP32 accumulation and FP32 master weights with Adam.  Parameters in
+ * this order: W1[64][12], b1[64], W2[64][64], b2[64], W3[2][64], b3[2]. */
+#define NRT_MLP_PARAMS 5122
+typedef struct nrt_mlp nrt_mlp;
+typedef struct {
+    int epochs;        /* passes over the samples (20) */
+    int batch;         /* samples per Adam step (>= 32) */
+    float lr;          /* Adam learning rate (1e-3) */
+    float beta1, beta2, eps; /* 0 = 0.9, 0.999, 1e-8 */
+    uint32_t seed;     /* shuffling seed */
+} nrt_train_opts;
+size_t nrt_mlp_param_count(void);
+int nrt_mlp_create(int device, uint32_t seed, nrt_mlp** out);   /* Glorot-uniform init */
+int nrt_mlp_destroy(nrt_mlp* mlp);
+int nrt_mlp_get_params(const nrt_mlp* mlp, float* host_params);  /* NRT_MLP_PARAMS floats */
+int nrt_mlp_set_params(nrt_mlp* mlp, const float* host_params);
+/* features: device n x 12 floats; out_uv: device n x 2 (unclamped network output). */
+int nrt_mlp_forward(const nrt_mlp* mlp, const float* features, int64_t n, float* out_uv, void* stream);
+/* Gradient of mean_i |y_i - t_i|^2 over the n rows (one batch), into host memory. */
+int nrt_mlp_gradients(nrt_mlp* mlp, const float* features, const float* targets, int64_t n, float* host_grads,
+                      float* host_loss, void* stream);
+/* Adam training on device samples; host_epoch_loss (optional) gets the mean batch loss per epoch. */
+int nrt_mlp_train(nrt_mlp* mlp, const float* features, const float* targets, int64_t n, const nrt_train_opts* opts,
+                  float* host_epoch_loss, void* stream);
+/* Versioned binary file with a CRC-32 (weights and Adam state). */
+int nrt_mlp_save(const nrt_mlp* mlp, const char* path);
+int nrt_mlp_load(const char* path, int device, nrt_mlp** out);
+/* Copy the network into the scene; enables NRT_INIT_LEARNED for it. */
+int nrt_scene_set_mlp(nrt_scene* scene, const nrt_mlp* mlp);
+/* Run the wavefront intersection with `opts` (which must use the midpoint
+ * guess) and record, for every solve that converged, its 12 features and its
+ * converged (u, v): training pairs for the network.  features: device
+ * capacity x 12, targets: device capacity x 2; *count gets the number of pairs
+ * found (it may exceed capacity; only capacity are written).  Synchronous. */
+int nrt_collect_training_data(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                              float* features, float* targets, int64_t capacity, int64_t* count, void* stream);
 
 const char* nrt_last_error(void);
 const char* nrt_version(void);

@@ -3,6 +3,7 @@
 
 #include <cstdint>
 
+#include "mlp.cuh"
 #include "patch_math.cuh"
 
 namespace nrt {
@@ -21,6 +22,7 @@ struct Scene {
     const float* cp;         // SoA blocks in patch-local homogeneous coordinates
     const float4* corners;   // per slot: four dehomogenised world-space corners q00, q10, q11, q01
     const float* delta;      // per slot: flatness (patchDelta) for flat-skip
+    const PatchFrame* frames;  // per slot: frame of the learned guess's features
     int n_slots;
 };
 
@@ -44,11 +46,18 @@ struct Opts {
     float flat_threshold;
     float cam_k;
     int counters;       // 1: accumulate all counters; 0: only the error count
+    int learned_iters;  // evaluations from the network's guess before the plain fallback
+    MlpParams mlp;      // network (init_mode 2)
+    float* col_feat;    // training-pair collection (null: off): capacity x 12
+    float* col_targ;    // capacity x 2
+    unsigned long long* col_count;
+    long long col_cap;
 };
 
 // Indices into the device counter block (nrt_counters order).
 enum Counter : int {
-    kRays = 0, kBoxTests, kCandidates, kCulled, kSolves, kEvals, kFp64Solves, kFp64Final, kHits, kErrors, kNumCounters
+    kRays = 0, kBoxTests, kCandidates, kCulled, kSolves, kEvals, kFp64Solves, kFp64Final, kHits, kErrors, kLearned,
+    kFallbacks, kNumCounters
 };
 // Followed by 64 per-degree evaluation counts and 64 per-degree hull-test counts.
 constexpr int kEvalsByDegree = kNumCounters, kHullByDegree = kNumCounters + 64, kCounterWords = kNumCounters + 128;

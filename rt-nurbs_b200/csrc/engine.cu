@@ -78,6 +78,65 @@ static float patch_delta(const float* P, int p, int q) {
     return d;
 }
 
+// Frame of the learned guess's features (see mlp.cuh): origin at the (0,0)
+// corner, axes the mean u- and v-chords A, B of the control net and the
+// normal of A x B scaled by sqrt|A x B|; all in patch-local coordinates.
+// Degenerate nets (collapsed edges) fall back to the box, normalised.
+static dev::PatchFrame patch_frame(const float* P, int p, int q, double cx, double cy, double cz, const Box3& b,
+                                   float delta) {
+    auto pt = [&](int i, int j, double o[3]) {
+        const float* c = P + 4 * (i * (q + 1) + j);
+        o[0] = c[0] / (double)c[3] - cx; o[1] = c[1] / (double)c[3] - cy; o[2] = c[2] / (double)c[3] - cz;
+    };
+    double A[3] = {0, 0, 0}, B[3] = {0, 0, 0}, o[3], t0[3], t1[3];
+    for (int j = 0; j <= q; ++j) {
+        pt(p, j, t1); pt(0, j, t0);
+        for (int k = 0; k < 3; ++k) A[k] += (t1[k] - t0[k]) / (q + 1);
+    }
+    for (int i = 0; i <= p; ++i) {
+        pt(i, q, t1); pt(i, 0, t0);
+        for (int k = 0; k < 3; ++k) B[k] += (t1[k] - t0[k]) / (p + 1);
+    }
+    pt(0, 0, o);
+    const double N[3] = {A[1] * B[2] - A[2] * B[1], A[2] * B[0] - A[0] * B[2], A[0] * B[1] - A[1] * B[0]};
+    const double nn = std::sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+    const double aa = A[0] * A[0] + A[1] * A[1] + A[2] * A[2], bb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+    dev::PatchFrame f{};
+    double M[3][3];  // columns A, B, N/sqrt|N|
+    double scale;
+    if (nn > 1e-9 * (aa + bb) && aa > 0 && bb > 0) {
+        const double s = 1.0 / std::sqrt(nn);
+        for (int k = 0; k < 3; ++k) { M[k][0] = A[k]; M[k][1] = B[k]; M[k][2] = N[k] * s; }
+        scale = std::sqrt(std::max(aa, bb));
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            o[k] = (double)b.lo[k] - (k == 0 ? cx : k == 1 ? cy : cz);
+            for (int l = 0; l < 3; ++l) M[k][l] = k == l ? std::max((double)b.hi[k] - b.lo[k], 1e-12) : 0.0;
+        }
+        scale = std::max({M[0][0], M[1][1], M[2][2]});
+    }
+    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+                       M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    const double id = 1.0 / det;
+    const double inv[9] = {(M[1][1] * M[2][2] - M[1][2] * M[2][1]) * id, (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id,
+                           (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id, (M[1][2] * M[2][0] - M[1][0] * M[2][2]) * id,
+                           (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id, (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id,
+                           (M[1][0] * M[2][1] - M[1][1] * M[2][0]) * id, (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id,
+                           (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id};
+    f.ox = (float)o[0]; f.oy = (float)o[1]; f.oz = (float)o[2];
+    for (int k = 0; k < 9; ++k) f.m[k] = (float)inv[k];
+    f.flat = (float)(delta / std::max(scale, 1e-30));
+    f.lo[0] = (float)(b.lo[0] - cx); f.lo[1] = (float)(b.lo[1] - cy); f.lo[2] = (float)(b.lo[2] - cz);
+    f.hi_x = (float)(b.hi[0] - cx); f.hi_y = (float)(b.hi[1] - cy); f.hi_z = (float)(b.hi[2] - cz);
+    return f;
+}
+
+dev::MlpParams blob_params(const void* blob);
+size_t mlp_blob_bytes();
+const void* mlp_device_blob(const nrt_mlp* m);
+int mlp_device(const nrt_mlp* m);
+
 }  // namespace nrt
 
 using namespace nrt;
@@ -100,6 +159,7 @@ struct nrt_scene {
     long long wf_chunk = 0;      // rays per wavefront pass
     int32_t* host_count = nullptr;  // pinned word for the per-round active count
     long long last_launches = 0, last_rounds = 0;  // of the last nrt_intersect
+    void* mlp_blob = nullptr;    // the scene's copy of the learned guess's network
 };
 
 
@@ -139,6 +199,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     std::vector<double4> centre(N);
     std::vector<float4> corners(4 * (size_t)N);
     std::vector<float> delta(N);
+    std::vector<dev::PatchFrame> frames(N);
     std::vector<float> blocks;
     std::vector<int32_t> slot_patch(N);
     size_t total_floats = 0;
@@ -182,6 +243,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
             corners[4 * (size_t)s + c] = make_float4(X[0] * iw, X[1] * iw, X[2] * iw, 0.f);
         }
         delta[s] = patch_delta(P, p, q);
+        frames[s] = patch_frame(P, p, q, cx, cy, cz, b, delta[s]);
         info.degree_hist[p * 8 + q] += 1;
         off += 4 * (size_t)np;
     }
@@ -192,8 +254,8 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
                  sz_cen = align(N * sizeof(double4)), sz_cp = align(blocks.size() * sizeof(float)),
                  sz_cor = align(corners.size() * sizeof(float4)), sz_del = align(N * sizeof(float)),
                  sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long)),
-                 sz_rank = align(N * sizeof(int32_t));
-    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank;
+                 sz_rank = align(N * sizeof(int32_t)), sz_frm = align(N * sizeof(dev::PatchFrame));
+    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank + sz_frm;
     // wavefront plan: patches ranked by (p, q, slot); one class per degree pair present
     std::vector<int32_t> by_rank(N), rank_of(N);
     for (int s2 = 0; s2 < N; ++s2) by_rank[s2] = s2;
@@ -239,6 +301,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     if (e == cudaSuccess) e = cudaMemset(sc->counters, 0, sz_ctr);
     at += sz_ctr;
     plan.rank_of = static_cast<const int32_t*>(put(rank_of.data(), N * sizeof(int32_t), sz_rank));
+    sc->view.frames = static_cast<const dev::PatchFrame*>(put(frames.data(), N * sizeof(dev::PatchFrame), sz_frm));
     sc->plan = plan;
     cudaSetDevice(prev);
     if (e != cudaSuccess) {
@@ -273,6 +336,12 @@ void to_dev_opts(const nrt_intersect_opts& o, dev::Opts& d, int counters) {
     d.flat_threshold = o.flat_threshold;
     d.cam_k = o.cam_k;
     d.counters = counters;
+    d.learned_iters = o.learned_iters;
+    d.mlp = dev::MlpParams{};
+    d.col_feat = nullptr;
+    d.col_targ = nullptr;
+    d.col_count = nullptr;
+    d.col_cap = 0;
 }
 
 }  // namespace
@@ -403,6 +472,7 @@ int nrt_scene_destroy(nrt_scene* scene) {
         if (e == cudaSuccess) e = e2;
     }
     if (scene->host_count) cudaFreeHost(scene->host_count);
+    if (scene->mlp_blob) cudaFree(scene->mlp_blob);
     cudaSetDevice(prev);
     delete scene;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFree(scene)");
@@ -456,8 +526,10 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     if (o.max_iter < 1 || o.max_iter > 256) return fail(NRT_ERR_INVALID, "max_iter %d outside 1..256", o.max_iter);
     if (!(o.eps > 0.f)) return fail(NRT_ERR_INVALID, "eps must be positive");
     if (o.init_mode != NRT_INIT_MIDPOINT && o.init_mode != NRT_INIT_BILINEAR) {
-        if (o.init_mode == NRT_INIT_LEARNED) return fail(NRT_ERR_UNSUPPORTED, "learned init needs a trained model");
-        return fail(NRT_ERR_INVALID, "unknown init mode %d", o.init_mode);
+        if (o.init_mode != NRT_INIT_LEARNED) return fail(NRT_ERR_INVALID, "unknown init mode %d", o.init_mode);
+        if (!scene->mlp_blob) return fail(NRT_ERR_INVALID, "learned init: no network set on this scene");
+        if (o.schedule != NRT_SCHED_WAVEFRONT)
+            return fail(NRT_ERR_UNSUPPORTED, "learned init runs on the wavefront schedule");
     }
     if (o.schedule != NRT_SCHED_PIXEL && o.schedule != NRT_SCHED_WAVEFRONT)
         return fail(NRT_ERR_INVALID, "unknown schedule %d", o.schedule);
@@ -469,6 +541,7 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     dev::Opts d;
     to_dev_opts(o, d, scene->counters_on);
+    if (scene->mlp_blob) d.mlp = blob_params(scene->mlp_blob);
     if (scene->counters_on)
         NRT_CUDA(cudaMemsetAsync(scene->counters, 0, dev::kCounterWords * sizeof(unsigned long long), st),
                  "counter reset");
@@ -544,6 +617,8 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
     out->fp64_final_steps = h[dev::kFp64Final];
     out->hits = h[dev::kHits];
     out->errors = h[dev::kErrors];
+    out->learned_solves = h[dev::kLearned];
+    out->learned_fallbacks = h[dev::kFallbacks];
     out->kernel_launches = (uint64_t)scene->last_launches;
     out->rounds = (uint64_t)scene->last_rounds;
     for (int k = 0; k < 64; ++k) {
@@ -630,3 +705,86 @@ void noalloc_record(nrt_scene* scene, long long launches, long long rounds) {
 }
 
 }  // namespace nrt
+
+extern "C" {
+
+int nrt_scene_set_mlp(nrt_scene* scene, const nrt_mlp* mlp) {
+    if (!scene || !mlp) return fail(NRT_ERR_INVALID, "null argument");
+    if (mlp_device(mlp) != scene->device) return fail(NRT_ERR_INVALID, "network and scene are on different devices");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != scene->device) cudaSetDevice(scene->device);
+    cudaError_t e = cudaSuccess;
+    if (!scene->mlp_blob) e = cudaMalloc(&scene->mlp_blob, mlp_blob_bytes());
+    if (e == cudaSuccess) e = cudaMemcpy(scene->mlp_blob, mlp_device_blob(mlp), mlp_blob_bytes(), cudaMemcpyDeviceToDevice);
+    if (prev != scene->device) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "scene network copy");
+    return NRT_OK;
+}
+
+int nrt_collect_training_data(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                              float* features, float* targets, int64_t capacity, int64_t* count, void* stream) {
+    if (!scene || !rays || !opts || !features || !targets || !count || n < 0 || capacity < 0)
+        return fail(NRT_ERR_INVALID, "bad argument");
+    if (opts->init_mode != NRT_INIT_MIDPOINT) return fail(NRT_ERR_INVALID, "training pairs come from the midpoint guess");
+    *count = 0;
+    if (n == 0) return NRT_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != scene->device) cudaSetDevice(scene->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // scratch outputs and the pair counter (this is a training-time call: it allocates)
+    void* tmp = nullptr;
+    const size_t out_bytes = (size_t)n * 16 + 256;
+    cudaError_t e = cudaMalloc(&tmp, out_bytes);
+    if (e != cudaSuccess) {
+        if (prev != scene->device) cudaSetDevice(prev);
+        return cuda_fail(e, "cudaMalloc(collection scratch)");
+    }
+    char* base = static_cast<char*>(tmp);
+    unsigned long long* dcount = reinterpret_cast<unsigned long long*>(base);
+    dev::Hits h{reinterpret_cast<int32_t*>(base + 256), reinterpret_cast<float*>(base + 256 + 4 * (size_t)n),
+                reinterpret_cast<float*>(base + 256 + 8 * (size_t)n), reinterpret_cast<float*>(base + 256 + 12 * (size_t)n),
+                nullptr, nullptr, nullptr};
+    e = cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), st);
+    dev::Opts d;
+    to_dev_opts(*opts, d, 0);
+    d.col_feat = features;
+    d.col_targ = targets;
+    d.col_count = dcount;
+    d.col_cap = capacity;
+    const dev::Rays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz};
+    const long long chunk = std::min<long long>(n, scene->wf_chunk);
+    if (e == cudaSuccess && scene->wf_rays < chunk) {
+        if (scene->wf_ws) cudaFree(scene->wf_ws);
+        scene->wf_ws = nullptr;
+        scene->wf_rays = 0;
+        e = cudaMalloc(&scene->wf_ws, dev::wavefront_scratch_bytes(chunk, scene->plan.n_slots));
+        if (e == cudaSuccess) scene->wf_rays = chunk;
+        else scene->wf_ws = nullptr;
+    }
+    if (e == cudaSuccess && !scene->host_count) e = cudaMallocHost(&scene->host_count, sizeof(int32_t));
+    long long launches = 0, rounds = 0;
+    if (e == cudaSuccess) {
+        const dev::WfBuffers wb = dev::wavefront_carve(scene->wf_ws, scene->wf_rays, scene->plan.n_slots);
+        for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
+            const long long m = std::min(chunk, (long long)n - at);
+            dev::Rays rc{r.ox + at, r.oy + at, r.oz + at, r.dx + at, r.dy + at, r.dz + at};
+            dev::Hits hc{h.patch + at, h.t + at, h.u + at, h.v + at, nullptr, nullptr, nullptr};
+            dev::Opts dc = d;
+            dc.seed_offset = d.seed_offset + (uint32_t)at;
+            e = dev::launch_wavefront(scene->view, scene->plan, rc, m, dc, hc, wb, scene->host_count, scene->counters, st,
+                                      &launches, &rounds);
+        }
+    }
+    unsigned long long got = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&got, dcount, sizeof(got), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    if (prev != scene->device) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "training-pair collection");
+    *count = (int64_t)got;
+    return NRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,732 @@
+// mlp.cu -- training and inference entry points of the learned-initial-guess
+// MLP (12 -> 64 -> 64 -> 2, SiLU), all on BF16 tensor cores (mma.sync
+// m16n8k16, FP32 accumulation) with FP32 master weights and Adam.
+//
+// Rounding points (mirrored by the CPU oracle, oracle/mlp_oracle.py): every
+// tensor-core operand is bfloat16 (inputs, weights, hidden activations, output
+// and hidden gradients); pre-activations, biases, bias gradients and weight
+// gradient accumulation are FP32.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <vector>
+
+#include "mlp.cuh"
+#include "nrt_internal.h"
+
+using namespace nrt::dev;
+
+namespace {
+
+constexpr int kP_W1 = 0, kP_B1 = kP_W1 + 64 * 12, kP_W2 = kP_B1 + 64, kP_B2 = kP_W2 + 64 * 64, kP_W3 = kP_B2 + 64,
+              kP_B3 = kP_W3 + 2 * 64, kNumParams = kP_B3 + 2;
+static_assert(kNumParams == NRT_MLP_PARAMS, "parameter count");
+
+// Byte offsets inside the device blob used by the kernels.
+constexpr size_t kB_W1 = 0, kB_W2 = kB_W1 + 64 * 16 * 2, kB_W3 = kB_W2 + 64 * 64 * 2, kB_B1 = kB_W3 + 8 * 64 * 2,
+                 kB_B2 = kB_B1 + 64 * 4, kB_B3 = kB_B2 + 64 * 4, kBlobBytes = kB_B3 + 8 * 4;
+
+}  // namespace
+
+namespace nrt {
+dev::MlpParams blob_params(const void* blob) {
+    const char* b = static_cast<const char*>(blob);
+    dev::MlpParams p;
+    p.w1t = reinterpret_cast<const __nv_bfloat16*>(b + kB_W1);
+    p.w2t = reinterpret_cast<const __nv_bfloat16*>(b + kB_W2);
+    p.w3t = reinterpret_cast<const __nv_bfloat16*>(b + kB_W3);
+    p.b1 = reinterpret_cast<const float*>(b + kB_B1);
+    p.b2 = reinterpret_cast<const float*>(b + kB_B2);
+    p.b3 = reinterpret_cast<const float*>(b + kB_B3);
+    return p;
+}
+size_t mlp_blob_bytes() { return kBlobBytes; }
+}  // namespace nrt
+
+struct nrt_mlp {
+    int device = 0;
+    float* master = nullptr;  // device, public order
+    float* m = nullptr;
+    float* v = nullptr;
+    float* grad = nullptr;
+    float* loss = nullptr;    // device scalar
+    void* blob = nullptr;     // device, kernel layout
+    long long step = 0;
+    std::vector<float> host_m, host_v;  // only used by save/load staging
+};
+
+namespace {
+
+// public index -> blob element, or -1 for none
+__device__ __forceinline__ void put_blob(char* blob, int k, float w) {
+    if (k < kP_B1) {
+        const int n = k / 12, i = k % 12;
+        reinterpret_cast<__nv_bfloat16*>(blob + kB_W1)[n * 16 + i] = __float2bfloat16_rn(w);
+    } else if (k < kP_W2) {
+        reinterpret_cast<float*>(blob + kB_B1)[k - kP_B1] = w;
+    } else if (k < kP_B2) {
+        reinterpret_cast<__nv_bfloat16*>(blob + kB_W2)[k - kP_W2] = __float2bfloat16_rn(w);
+    } else if (k < kP_W3) {
+        reinterpret_cast<float*>(blob + kB_B2)[k - kP_B2] = w;
+    } else if (k < kP_B3) {
+        reinterpret_cast<__nv_bfloat16*>(blob + kB_W3)[k - kP_W3] = __float2bfloat16_rn(w);
+    } else {
+        reinterpret_cast<float*>(blob + kB_B3)[k - kP_B3] = w;
+    }
+}
+
+__global__ void k_mlp_to_blob(const float* master, char* blob) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < kNumParams) put_blob(blob, k, master[k]);
+}
+
+__global__ void k_mlp_adam(float* master, float* m, float* v, float* grad, char* blob, float lr, float b1, float b2,
+                           float eps, float bc1, float bc2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kNumParams) return;
+    const float g = grad[k];
+    const float mk = b1 * m[k] + (1.f - b1) * g;
+    const float vk = b2 * v[k] + (1.f - b2) * g * g;
+    m[k] = mk;
+    v[k] = vk;
+    const float w = master[k] - lr * (mk / bc1) / (sqrtf(vk / bc2) + eps);
+    master[k] = w;
+    grad[k] = 0.f;
+    put_blob(blob, k, w);
+}
+
+struct TrainWarp {
+    __nv_bfloat16 x[32][kMlpLdIn];
+    __nv_bfloat16 h1[32][kMlpLd], h2[32][kMlpLd], dz[32][kMlpLd];
+    __nv_bfloat16 dy[32][kMlpLdIn];
+    float z1[32][64], z2[32][64];
+    float t[32][2];
+};
+
+struct TrainSmem {
+    __nv_bfloat16 w1t[64][kMlpLdIn], w2t[64][kMlpLd], w3t[8][kMlpLd];
+    float b1[64], b2[64], b3[8];
+    float gw1[64][16], gb1[64], gw2[64][64], gb2[64], gw3[8][64], gb3[8];
+    float loss;
+    TrainWarp w[4];
+};
+
+__device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
+
+// Sum a value over the 8 lanes that share threadIdx & 3 (the rows of a fragment column).
+__device__ __forceinline__ float sum_over_rows(float x) {
+    x += __shfl_xor_sync(0xffffffffu, x, 4);
+    x += __shfl_xor_sync(0xffffffffu, x, 8);
+    x += __shfl_xor_sync(0xffffffffu, x, 16);
+    return x;
+}
+
+// Forward + backward over `count` samples starting at `begin` (through perm if
+// given); weight and bias gradients of mean((Y-T)^2) summed into grad (public
+// order), the batch loss into *loss.  Blocks of 4 warps, 32 samples per warp.
+__global__ void __launch_bounds__(128) k_mlp_fwd_bwd(MlpParams P, const float* __restrict__ X,
+                                                     const float* __restrict__ T, const int32_t* __restrict__ perm,
+                                                     long long begin, long long count, float inv_batch, float* grad,
+                                                     float* loss) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+    for (int k = threadIdx.x; k < 64 * 16; k += blockDim.x) s.w1t[k / 16][k % 16] = P.w1t[k];
+    for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) s.w2t[k / 64][k % 64] = P.w2t[k];
+    for (int k = threadIdx.x; k < 8 * 64; k += blockDim.x) s.w3t[k / 64][k % 64] = P.w3t[k];
+    for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+        s.b1[k] = P.b1[k];
+        s.b2[k] = P.b2[k];
+        s.gb1[k] = 0.f;
+        s.gb2[k] = 0.f;
+    }
+    for (int k = threadIdx.x; k < 8; k += blockDim.x) {
+        s.b3[k] = P.b3[k];
+        s.gb3[k] = 0.f;
+    }
+    for (int k = threadIdx.x; k < 64 * 16; k += blockDim.x) (&s.gw1[0][0])[k] = 0.f;
+    for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) (&s.gw2[0][0])[k] = 0.f;
+    for (int k = threadIdx.x; k < 8 * 64; k += blockDim.x) (&s.gw3[0][0])[k] = 0.f;
+    if (threadIdx.x == 0) s.loss = 0.f;
+    __syncthreads();
+    TrainWarp& W = s.w[warp];
+    const long long tiles = (count + 31) / 32;
+    float my_loss = 0.f;
+    for (long long tile = (long long)blockIdx.x * 4 + warp; tile < tiles; tile += (long long)gridDim.x * 4) {
+        const long long row = tile * 32 + lane;
+        const bool valid = row < count;
+        const long long smp = valid ? (perm ? (long long)perm[begin + row] : begin + row) : 0;
+#pragma unroll
+        for (int k = 0; k < 16; k += 2) {
+            const float a = (valid && k < 12) ? X[smp * 12 + k] : 0.f;
+            const float b = (valid && k + 1 < 12) ? X[smp * 12 + k + 1] : 0.f;
+            *reinterpret_cast<uint32_t*>(&W.x[lane][k]) = pack_bf16(a, b);
+        }
+        W.t[lane][0] = valid ? T[smp * 2] : 0.f;
+        W.t[lane][1] = valid ? T[smp * 2 + 1] : 0.f;
+        for (int k = 0; k < 16; ++k) W.dy[lane][k] = __float2bfloat16_rn(0.f);
+        __syncwarp();
+        // ---- forward: layer 1 (K = 16) and layer 2 (K = 64), keeping the pre-activations
+#pragma unroll
+        for (int layer = 0; layer < 2; ++layer) {
+            float acc[2][8][4];
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 8; ++nt) {
+                    acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.f;
+                    const int ksteps = layer == 0 ? 1 : 4;
+                    for (int ks = 0; ks < ksteps; ++ks) {
+                        const int r0 = mt * 16, c0 = ks * 16;
+                        uint32_t a0, a1, a2, a3, b0, b1;
+                        if (layer == 0) {
+                            a0 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][c0 + 2 * t4]);
+                            a1 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][c0 + 2 * t4]);
+                            a2 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][c0 + 2 * t4 + 8]);
+                            a3 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][c0 + 2 * t4 + 8]);
+                            b0 = *reinterpret_cast<const uint32_t*>(&s.w1t[nt * 8 + g][c0 + 2 * t4]);
+                            b1 = *reinterpret_cast<const uint32_t*>(&s.w1t[nt * 8 + g][c0 + 2 * t4 + 8]);
+                        } else {
+                            a0 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g][c0 + 2 * t4]);
+                            a1 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g + 8][c0 + 2 * t4]);
+                            a2 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g][c0 + 2 * t4 + 8]);
+                            a3 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g + 8][c0 + 2 * t4 + 8]);
+                            b0 = *reinterpret_cast<const uint32_t*>(&s.w2t[nt * 8 + g][c0 + 2 * t4]);
+                            b1 = *reinterpret_cast<const uint32_t*>(&s.w2t[nt * 8 + g][c0 + 2 * t4 + 8]);
+                        }
+                        mma_bf16(acc[mt][nt], a0, a1, a2, a3, b0, b1);
+                    }
+                }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 8; ++nt) {
+                    const int col = nt * 8 + 2 * t4, r = mt * 16 + g;
+                    const float* bias = layer == 0 ? s.b1 : s.b2;
+                    float(*z)[64] = layer == 0 ? W.z1 : W.z2;
+                    __nv_bfloat16(*h)[kMlpLd] = layer == 0 ? W.h1 : W.h2;
+                    const float v0 = acc[mt][nt][0] + bias[col], v1 = acc[mt][nt][1] + bias[col + 1];
+                    const float v2 = acc[mt][nt][2] + bias[col], v3 = acc[mt][nt][3] + bias[col + 1];
+                    z[r][col] = v0; z[r][col + 1] = v1; z[r + 8][col] = v2; z[r + 8][col + 1] = v3;
+                    *reinterpret_cast<uint32_t*>(&h[r][col]) = pack_bf16(silu(v0), silu(v1));
+                    *reinterpret_cast<uint32_t*>(&h[r + 8][col]) = pack_bf16(silu(v2), silu(v3));
+                }
+            __syncwarp();
+        }
+        // ---- output layer and dY = 2 (Y - T) / B
+        {
+            float gb3_0 = 0.f, gb3_1 = 0.f;
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {
+                    const int r0 = mt * 16, c0 = ks * 16;
+                    mma_bf16(d, *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g][c0 + 2 * t4]),
+                             *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g + 8][c0 + 2 * t4]),
+                             *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g][c0 + 2 * t4 + 8]),
+                             *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g + 8][c0 + 2 * t4 + 8]),
+                             *reinterpret_cast<const uint32_t*>(&s.w3t[g][c0 + 2 * t4]),
+                             *reinterpret_cast<const uint32_t*>(&s.w3t[g][c0 + 2 * t4 + 8]));
+                }
+                if (t4 == 0) {  // columns 0 and 1 are the real outputs
+                    const int r = mt * 16 + g;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int rr = r + 8 * h;
+                        const bool ok = tile * 32 + rr < count;
+                        const float y0 = d[2 * h] + s.b3[0], y1 = d[2 * h + 1] + s.b3[1];
+                        const float e0 = ok ? y0 - W.t[rr][0] : 0.f, e1 = ok ? y1 - W.t[rr][1] : 0.f;
+                        my_loss += e0 * e0 + e1 * e1;
+                        const float d0 = 2.f * e0 * inv_batch, d1 = 2.f * e1 * inv_batch;
+                        gb3_0 += d0;
+                        gb3_1 += d1;
+                        *reinterpret_cast<uint32_t*>(&W.dy[rr][0]) = pack_bf16(d0, d1);
+                    }
+                }
+            }
+            gb3_0 = sum_over_rows(gb3_0);
+            gb3_1 = sum_over_rows(gb3_1);
+            if (lane == 0) {
+                atomicAdd(&s.gb3[0], gb3_0);
+                atomicAdd(&s.gb3[1], gb3_1);
+            }
+        }
+        __syncwarp();
+        // ---- dW3 = dY^T H2  (M = outputs 0..15, N = 64, K = 32 rows)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                const int k0 = ks * 16 + 2 * t4;
+                const uint32_t a0 = pack_bf16(bf(W.dy[k0][g]), bf(W.dy[k0 + 1][g]));
+                const uint32_t a1 = pack_bf16(bf(W.dy[k0][g + 8]), bf(W.dy[k0 + 1][g + 8]));
+                const uint32_t a2 = pack_bf16(bf(W.dy[k0 + 8][g]), bf(W.dy[k0 + 9][g]));
+                const uint32_t a3 = pack_bf16(bf(W.dy[k0 + 8][g + 8]), bf(W.dy[k0 + 9][g + 8]));
+                const uint32_t b0 = pack_bf16(bf(W.h2[k0][nt * 8 + g]), bf(W.h2[k0 + 1][nt * 8 + g]));
+                const uint32_t b1 = pack_bf16(bf(W.h2[k0 + 8][nt * 8 + g]), bf(W.h2[k0 + 9][nt * 8 + g]));
+                mma_bf16(d, a0, a1, a2, a3, b0, b1);
+            }
+            if (g < 8) {
+                atomicAdd(&s.gw3[g][nt * 8 + 2 * t4], d[0]);
+                atomicAdd(&s.gw3[g][nt * 8 + 2 * t4 + 1], d[1]);
+            }
+        }
+        // ---- dH2 = dY W3, dZ2 = dH2 * silu'(Z2)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+                const int r0 = mt * 16;
+                const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g][2 * t4]);
+                const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g + 8][2 * t4]);
+                const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g][2 * t4 + 8]);
+                const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g + 8][2 * t4 + 8]);
+                const uint32_t b0 = pack_bf16(bf(s.w3t[2 * t4][nt * 8 + g]), bf(s.w3t[2 * t4 + 1][nt * 8 + g]));
+                const uint32_t b1 = 0u;  // output rows 8..15 do not exist
+                mma_bf16(d, a0, a1, a2, a3, b0, b1);
+                const int col = nt * 8 + 2 * t4, r = r0 + g;
+                float dz[4];
+                dz[0] = d[0] * dsilu_f(W.z2[r][col]);
+                dz[1] = d[1] * dsilu_f(W.z2[r][col + 1]);
+                dz[2] = d[2] * dsilu_f(W.z2[r + 8][col]);
+                dz[3] = d[3] * dsilu_f(W.z2[r + 8][col + 1]);
+                *reinterpret_cast<uint32_t*>(&W.dz[r][col]) = pack_bf16(dz[0], dz[1]);
+                *reinterpret_cast<uint32_t*>(&W.dz[r + 8][col]) = pack_bf16(dz[2], dz[3]);
+                const float c0 = sum_over_rows(dz[0] + dz[2]), c1 = sum_over_rows(dz[1] + dz[3]);
+                if (g == 0) {
+                    atomicAdd(&s.gb2[col], c0);
+                    atomicAdd(&s.gb2[col + 1], c1);
+                }
+            }
+        __syncwarp();
+        // ---- dW2 = dZ2^T H1 (M = 64, N = 64, K = 32 rows)
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int ks = 0; ks < 2; ++ks) {
+                    const int k0 = ks * 16 + 2 * t4, m0 = mt * 16 + g, n0 = nt * 8 + g;
+                    const uint32_t a0 = pack_bf16(bf(W.dz[k0][m0]), bf(W.dz[k0 + 1][m0]));
+                    const uint32_t a1 = pack_bf16(bf(W.dz[k0][m0 + 8]), bf(W.dz[k0 + 1][m0 + 8]));
+                    const uint32_t a2 = pack_bf16(bf(W.dz[k0 + 8][m0]), bf(W.dz[k0 + 9][m0]));
+                    const uint32_t a3 = pack_bf16(bf(W.dz[k0 + 8][m0 + 8]), bf(W.dz[k0 + 9][m0 + 8]));
+                    const uint32_t b0 = pack_bf16(bf(W.h1[k0][n0]), bf(W.h1[k0 + 1][n0]));
+                    const uint32_t b1 = pack_bf16(bf(W.h1[k0 + 8][n0]), bf(W.h1[k0 + 9][n0]));
+                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
+                }
+                const int m = mt * 16 + g, n = nt * 8 + 2 * t4;
+                atomicAdd(&s.gw2[m][n], d[0]);
+                atomicAdd(&s.gw2[m][n + 1], d[1]);
+                atomicAdd(&s.gw2[m + 8][n], d[2]);
+                atomicAdd(&s.gw2[m + 8][n + 1], d[3]);
+            }
+        // ---- dH1 = dZ2 W2, then dZ1 = dH1 * silu'(Z1) (overwrites dz after all reads)
+        float dh1[2][8][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                dh1[mt][nt][0] = dh1[mt][nt][1] = dh1[mt][nt][2] = dh1[mt][nt][3] = 0.f;
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {
+                    const int r0 = mt * 16, c0 = ks * 16, k0 = c0 + 2 * t4, n0 = nt * 8 + g;
+                    const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g][k0]);
+                    const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g + 8][k0]);
+                    const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g][k0 + 8]);
+                    const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g + 8][k0 + 8]);
+                    const uint32_t b0 = pack_bf16(bf(s.w2t[k0][n0]), bf(s.w2t[k0 + 1][n0]));
+                    const uint32_t b1 = pack_bf16(bf(s.w2t[k0 + 8][n0]), bf(s.w2t[k0 + 9][n0]));
+                    mma_bf16(dh1[mt][nt], a0, a1, a2, a3, b0, b1);
+                }
+            }
+        __syncwarp();
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int col = nt * 8 + 2 * t4, r = mt * 16 + g;
+                float dz[4];
+                dz[0] = dh1[mt][nt][0] * dsilu_f(W.z1[r][col]);
+                dz[1] = dh1[mt][nt][1] * dsilu_f(W.z1[r][col + 1]);
+                dz[2] = dh1[mt][nt][2] * dsilu_f(W.z1[r + 8][col]);
+                dz[3] = dh1[mt][nt][3] * dsilu_f(W.z1[r + 8][col + 1]);
+                *reinterpret_cast<uint32_t*>(&W.dz[r][col]) = pack_bf16(dz[0], dz[1]);
+                *reinterpret_cast<uint32_t*>(&W.dz[r + 8][col]) = pack_bf16(dz[2], dz[3]);
+                const float c0 = sum_over_rows(dz[0] + dz[2]), c1 = sum_over_rows(dz[1] + dz[3]);
+                if (g == 0) {
+                    atomicAdd(&s.gb1[col], c0);
+                    atomicAdd(&s.gb1[col + 1], c1);
+                }
+            }
+        __syncwarp();
+        // ---- dW1 = dZ1^T X (M = 64, N = 16, K = 32 rows)
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int ks = 0; ks < 2; ++ks) {
+                    const int k0 = ks * 16 + 2 * t4, m0 = mt * 16 + g, n0 = nt * 8 + g;
+                    const uint32_t a0 = pack_bf16(bf(W.dz[k0][m0]), bf(W.dz[k0 + 1][m0]));
+                    const uint32_t a1 = pack_bf16(bf(W.dz[k0][m0 + 8]), bf(W.dz[k0 + 1][m0 + 8]));
+                    const uint32_t a2 = pack_bf16(bf(W.dz[k0 + 8][m0]), bf(W.dz[k0 + 9][m0]));
+                    const uint32_t a3 = pack_bf16(bf(W.dz[k0 + 8][m0 + 8]), bf(W.dz[k0 + 9][m0 + 8]));
+                    const uint32_t b0 = pack_bf16(bf(W.x[k0][n0]), bf(W.x[k0 + 1][n0]));
+                    const uint32_t b1 = pack_bf16(bf(W.x[k0 + 8][n0]), bf(W.x[k0 + 9][n0]));
+                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
+                }
+                const int m = mt * 16 + g, n = nt * 8 + 2 * t4;
+                atomicAdd(&s.gw1[m][n], d[0]);
+                atomicAdd(&s.gw1[m][n + 1], d[1]);
+                atomicAdd(&s.gw1[m + 8][n], d[2]);
+                atomicAdd(&s.gw1[m + 8][n + 1], d[3]);
+            }
+        __syncwarp();
+    }
+    my_loss = sum_over_rows(my_loss);
+    my_loss += __shfl_xor_sync(0xffffffffu, my_loss, 1);
+    my_loss += __shfl_xor_sync(0xffffffffu, my_loss, 2);
+    if (lane == 0) atomicAdd(&s.loss, my_loss);
+    __syncthreads();
+    for (int k = threadIdx.x; k < kNumParams; k += blockDim.x) {
+        float v;
+        if (k < kP_B1) v = s.gw1[k / 12][k % 12];
+        else if (k < kP_W2) v = s.gb1[k - kP_B1];
+        else if (k < kP_B2) v = (&s.gw2[0][0])[k - kP_W2];
+        else if (k < kP_W3) v = s.gb2[k - kP_B2];
+        else if (k < kP_B3) v = (&s.gw3[0][0])[k - kP_W3];
+        else v = s.gb3[k - kP_B3];
+        if (v != 0.f) atomicAdd(grad + k, v);
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, s.loss * inv_batch);
+}
+
+// Inference on feature rows (n x 12) -> outputs (n x 2), unclamped.
+__global__ void __launch_bounds__(256) k_mlp_forward(MlpParams P, const float* __restrict__ X, long long n,
+                                                     float* __restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw);
+    mlp_load(s, P);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (long long base = ((long long)blockIdx.x * 8 + warp) * 32; base < n; base += (long long)gridDim.x * 256) {
+        const long long r = base + lane;
+        float x[kMlpIn];
+#pragma unroll
+        for (int k = 0; k < kMlpIn; ++k) x[k] = r < n ? X[r * 12 + k] : 0.f;
+        float u, v;
+        mlp_infer_warp(s, warp, lane, x, u, v);
+        if (r < n) {
+            Y[2 * r] = u;
+            Y[2 * r + 1] = v;
+        }
+    }
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return nrt::fail(e == cudaErrorMemoryAllocation ? NRT_ERR_NOMEM : NRT_ERR_CUDA, "%s: %s", what,
+                     cudaGetErrorString(e));
+}
+
+uint32_t crc32(const void* data, size_t n) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    uint32_t c = 0xFFFFFFFFu;
+    for (size_t i = 0; i < n; ++i) {
+        c ^= p[i];
+        for (int k = 0; k < 8; ++k) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
+    }
+    return ~c;
+}
+
+int upload_blob(nrt_mlp* m) {
+    k_mlp_to_blob<<<(kNumParams + 255) / 256, 256>>>(m->master, static_cast<char*>(m->blob));
+    const cudaError_t e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? NRT_OK : cuda_fail(e, "mlp weights");
+}
+
+struct DeviceGuard {
+    int prev = 0;
+    bool changed = false;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) {
+            cudaSetDevice(dev);
+            changed = true;
+        }
+    }
+    ~DeviceGuard() {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+size_t nrt_mlp_param_count(void) { return kNumParams; }
+
+int nrt_mlp_create(int device, uint32_t seed, nrt_mlp** out) {
+    if (!out) return nrt::fail(NRT_ERR_INVALID, "out is null");
+    *out = nullptr;
+    nrt_mlp* m = new (std::nothrow) nrt_mlp();
+    if (!m) return nrt::fail(NRT_ERR_NOMEM, "host allocation failed");
+    m->device = device;
+    DeviceGuard dg(device);
+    const size_t pbytes = sizeof(float) * kNumParams;
+    cudaError_t e = cudaMalloc(&m->master, pbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&m->m, pbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&m->v, pbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&m->grad, pbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&m->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->blob, kBlobBytes);
+    if (e == cudaSuccess) e = cudaMemset(m->blob, 0, kBlobBytes);
+    if (e == cudaSuccess) e = cudaMemset(m->m, 0, pbytes);
+    if (e == cudaSuccess) e = cudaMemset(m->v, 0, pbytes);
+    if (e == cudaSuccess) e = cudaMemset(m->grad, 0, pbytes);
+    if (e != cudaSuccess) {
+        nrt_mlp_destroy(m);
+        return cuda_fail(e, "mlp allocation");
+    }
+    // Glorot-uniform weights from a seeded generator, zero biases
+    std::vector<float> w(kNumParams, 0.f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int fan_out, int fan_in) {
+        const float a = std::sqrt(6.f / (float)(fan_in + fan_out));
+        std::uniform_real_distribution<float> U(-a, a);
+        for (int k = 0; k < fan_out * fan_in; ++k) w[off + k] = U(rng);
+    };
+    fill(kP_W1, 64, 12);
+    fill(kP_W2, 64, 64);
+    fill(kP_W3, 2, 64);
+    w[kP_B3] = 0.5f;  // outputs start at the patch midpoint
+    w[kP_B3 + 1] = 0.5f;
+    e = cudaMemcpy(m->master, w.data(), pbytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        nrt_mlp_destroy(m);
+        return cuda_fail(e, "mlp upload");
+    }
+    if (int st = upload_blob(m)) {
+        nrt_mlp_destroy(m);
+        return st;
+    }
+    *out = m;
+    return NRT_OK;
+}
+
+int nrt_mlp_destroy(nrt_mlp* m) {
+    if (!m) return NRT_OK;
+    DeviceGuard dg(m->device);
+    cudaFree(m->master);
+    cudaFree(m->m);
+    cudaFree(m->v);
+    cudaFree(m->grad);
+    cudaFree(m->loss);
+    cudaFree(m->blob);
+    delete m;
+    return NRT_OK;
+}
+
+int nrt_mlp_get_params(const nrt_mlp* m, float* host_out) {
+    if (!m || !host_out) return nrt::fail(NRT_ERR_INVALID, "null argument");
+    DeviceGuard dg(m->device);
+    const cudaError_t e = cudaMemcpy(host_out, m->master, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? NRT_OK : cuda_fail(e, "mlp params");
+}
+
+int nrt_mlp_set_params(nrt_mlp* m, const float* host_in) {
+    if (!m || !host_in) return nrt::fail(NRT_ERR_INVALID, "null argument");
+    DeviceGuard dg(m->device);
+    const cudaError_t e = cudaMemcpy(m->master, host_in, sizeof(float) * kNumParams, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp params");
+    return upload_blob(m);
+}
+
+int nrt_mlp_forward(const nrt_mlp* m, const float* features, int64_t n, float* out_uv, void* stream) {
+    if (!m || (n > 0 && (!features || !out_uv)) || n < 0) return nrt::fail(NRT_ERR_INVALID, "bad argument");
+    if (n == 0) return NRT_OK;
+    DeviceGuard dg(m->device);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+        attr_set = true;
+    }
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_mlp_forward<<<(unsigned)blocks, 256, sizeof(MlpSmem), static_cast<cudaStream_t>(stream)>>>(
+        nrt::blob_params(m->blob), features, n, out_uv);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? NRT_OK : cuda_fail(e, "mlp forward");
+}
+
+static int fwd_bwd(nrt_mlp* m, const float* X, const float* T, const int32_t* perm, long long begin, long long count,
+                   long long batch, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_mlp_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
+        attr_set = true;
+    }
+    const long long tiles = (count + 31) / 32;
+    long long blocks = (tiles + 3) / 4;
+    if (blocks > 148) blocks = 148;
+    k_mlp_fwd_bwd<<<(unsigned)blocks, 128, sizeof(TrainSmem), st>>>(nrt::blob_params(m->blob), X, T, perm, begin, count,
+                                                                      1.f / (float)batch, m->grad, m->loss);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? NRT_OK : cuda_fail(e, "mlp fwd/bwd");
+}
+
+int nrt_mlp_gradients(nrt_mlp* m, const float* features, const float* targets, int64_t n, float* host_grads,
+                      float* host_loss, void* stream) {
+    if (!m || !features || !targets || n <= 0 || !host_grads) return nrt::fail(NRT_ERR_INVALID, "bad argument");
+    DeviceGuard dg(m->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(m->grad, 0, sizeof(float) * kNumParams, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->loss, 0, sizeof(float), st);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp grad reset");
+    if (int s2 = fwd_bwd(m, features, targets, nullptr, 0, n, n, st)) return s2;
+    e = cudaMemcpyAsync(host_grads, m->grad, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost, st);
+    float loss = 0.f;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->grad, 0, sizeof(float) * kNumParams, st);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp gradients");
+    if (host_loss) *host_loss = loss;
+    return NRT_OK;
+}
+
+int nrt_mlp_train(nrt_mlp* m, const float* features, const float* targets, int64_t n, const nrt_train_opts* o,
+                  float* host_epoch_loss, void* stream) {
+    if (!m || !features || !targets || n <= 0 || !o) return nrt::fail(NRT_ERR_INVALID, "bad argument");
+    if (o->epochs < 1 || o->batch < 32 || !(o->lr > 0.f)) return nrt::fail(NRT_ERR_INVALID, "bad training options");
+    if (n > (int64_t)INT32_MAX) return nrt::fail(NRT_ERR_INVALID, "too many samples");
+    DeviceGuard dg(m->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int32_t* perm = nullptr;
+    cudaError_t e = cudaMalloc(&perm, sizeof(int32_t) * n);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(permutation)");
+    std::vector<int32_t> idx(n);
+    for (int64_t k = 0; k < n; ++k) idx[k] = (int32_t)k;
+    std::mt19937_64 rng(o->seed);
+    int status = NRT_OK;
+    const float b1 = o->beta1 > 0 ? o->beta1 : 0.9f, b2 = o->beta2 > 0 ? o->beta2 : 0.999f,
+                ep = o->eps > 0 ? o->eps : 1e-8f;
+    for (int epoch = 0; epoch < o->epochs && status == NRT_OK; ++epoch) {
+        std::shuffle(idx.begin(), idx.end(), rng);
+        e = cudaMemcpyAsync(perm, idx.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(m->loss, 0, sizeof(float), st);
+        if (e != cudaSuccess) { status = cuda_fail(e, "epoch setup"); break; }
+        long long batches = 0;
+        for (long long b = 0; b < n && status == NRT_OK; b += o->batch) {
+            const long long cnt = std::min<long long>(o->batch, n - b);
+            status = fwd_bwd(m, features, targets, perm, b, cnt, cnt, st);
+            ++m->step;
+            const float bc1 = 1.f - std::pow(b1, (float)m->step), bc2 = 1.f - std::pow(b2, (float)m->step);
+            k_mlp_adam<<<(kNumParams + 255) / 256, 256, 0, st>>>(m->master, m->m, m->v, m->grad,
+                                                                 static_cast<char*>(m->blob), o->lr, b1, b2, ep, bc1,
+                                                                 bc2);
+            ++batches;
+        }
+        float loss = 0.f;
+        e = cudaMemcpyAsync(&loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { status = cuda_fail(e, "epoch loss"); break; }
+        if (host_epoch_loss) host_epoch_loss[epoch] = loss / (float)batches;
+    }
+    cudaFree(perm);
+    return status;
+}
+
+// File: "NRTMLP01", u32 version 1, u32 dims 12/64/64/2, u32 parameter count,
+// i64 Adam step, master weights, Adam m, Adam v (float32), u32 CRC-32 of all
+// preceding bytes.
+int nrt_mlp_save(const nrt_mlp* m, const char* path) {
+    if (!m || !path) return nrt::fail(NRT_ERR_INVALID, "null argument");
+    DeviceGuard dg(m->device);
+    std::vector<float> w(kNumParams), mm(kNumParams), vv(kNumParams);
+    cudaError_t e = cudaMemcpy(w.data(), m->master, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(mm.data(), m->m, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(vv.data(), m->v, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp save");
+    std::vector<unsigned char> buf;
+    auto put = [&](const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        buf.insert(buf.end(), c, c + n);
+    };
+    const uint32_t hdr[6] = {1, 12, 64, 64, 2, (uint32_t)kNumParams};
+    put("NRTMLP01", 8);
+    put(hdr, sizeof(hdr));
+    const int64_t step = m->step;
+    put(&step, sizeof(step));
+    put(w.data(), sizeof(float) * kNumParams);
+    put(mm.data(), sizeof(float) * kNumParams);
+    put(vv.data(), sizeof(float) * kNumParams);
+    const uint32_t crc = crc32(buf.data(), buf.size());
+    put(&crc, sizeof(crc));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return nrt::fail(NRT_ERR_INVALID, "cannot open %s for writing", path);
+    const size_t wrote = std::fwrite(buf.data(), 1, buf.size(), f);
+    const int closed = std::fclose(f);
+    if (wrote != buf.size() || closed != 0) return nrt::fail(NRT_ERR_INVALID, "short write to %s", path);
+    return NRT_OK;
+}
+
+int nrt_mlp_load(const char* path, int device, nrt_mlp** out) {
+    if (!path || !out) return nrt::fail(NRT_ERR_INVALID, "null argument");
+    *out = nullptr;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return nrt::fail(NRT_ERR_INVALID, "cannot open %s", path);
+    std::vector<unsigned char> buf;
+    unsigned char tmp[65536];
+    size_t got;
+    while ((got = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
+    std::fclose(f);
+    const size_t expect = 8 + 24 + 8 + 3 * sizeof(float) * kNumParams + 4;
+    if (buf.size() != expect || std::memcmp(buf.data(), "NRTMLP01", 8) != 0)
+        return nrt::fail(NRT_ERR_INVALID, "%s is not an nrt MLP file", path);
+    uint32_t crc;
+    std::memcpy(&crc, buf.data() + buf.size() - 4, 4);
+    if (crc != crc32(buf.data(), buf.size() - 4)) return nrt::fail(NRT_ERR_INVALID, "%s: checksum mismatch", path);
+    uint32_t hdr[6];
+    std::memcpy(hdr, buf.data() + 8, sizeof(hdr));
+    if (hdr[0] != 1 || hdr[1] != 12 || hdr[2] != 64 || hdr[3] != 64 || hdr[4] != 2 || hdr[5] != (uint32_t)kNumParams)
+        return nrt::fail(NRT_ERR_INVALID, "%s: unsupported version or shape", path);
+    nrt_mlp* m = nullptr;
+    if (int st = nrt_mlp_create(device, 0, &m)) return st;
+    int64_t step;
+    std::memcpy(&step, buf.data() + 32, 8);
+    m->step = step;
+    const unsigned char* p = buf.data() + 40;
+    DeviceGuard dg(device);
+    cudaError_t e = cudaMemcpy(m->master, p, sizeof(float) * kNumParams, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(m->m, p + sizeof(float) * kNumParams, sizeof(float) * kNumParams, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(m->v, p + 2 * sizeof(float) * kNumParams, sizeof(float) * kNumParams, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        nrt_mlp_destroy(m);
+        return cuda_fail(e, "mlp load");
+    }
+    if (int st = upload_blob(m)) {
+        nrt_mlp_destroy(m);
+        return st;
+    }
+    *out = m;
+    return NRT_OK;
+}
+
+}  // extern "C"
+
+namespace nrt {
+const void* mlp_device_blob(const nrt_mlp* m) { return m ? m->blob : nullptr; }
+int mlp_device(const nrt_mlp* m) { return m ? m->device : -1; }
+}  // namespace nrt

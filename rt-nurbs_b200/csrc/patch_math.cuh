@@ -231,6 +231,69 @@ __device__ __forceinline__ bool hull_misses(const float* __restrict__ blk, const
     return pos1 | neg1 | pos2 | neg2;
 }
 
+// Subdivided hull test.  The patch's plane residuals n_k.S + e_k are rational
+// Bezier functions whose homogeneous coefficients are a = n1.P + e1*w and
+// b = n2.P + e2*w.  Splitting the coefficient net at u = 1/2 (each column
+// independently) gives the two halves' nets, whose hulls are tighter than the
+// whole net's; likewise at v = 1/2 (each row).  If both halves of either split
+// lie beyond +lim or below -lim for one plane, no evaluation point in [0,1]^2
+// can meet the stop rule and Newton's outcome is "no hit".  Columns and rows
+// stream from memory one at a time, so no 2D intermediate is held.
+template <int M>
+__device__ __forceinline__ void half_flags(const float (&a)[M + 1], const float (&b)[M + 1], const float (&w)[M + 1],
+                                           float lim, bool (&f)[2][4]) {
+    float ta[M + 1], tb[M + 1], tw[M + 1];
+#pragma unroll
+    for (int i = 0; i <= M; ++i) { ta[i] = a[i]; tb[i] = b[i]; tw[i] = w[i]; }
+    auto upd = [&](int h, float x, float y, float ww) {
+        const float m = lim * ww;
+        f[h][0] &= x > m; f[h][1] &= x < -m; f[h][2] &= y > m; f[h][3] &= y < -m;
+    };
+    upd(0, ta[0], tb[0], tw[0]);
+    upd(1, ta[M], tb[M], tw[M]);
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+#pragma unroll
+        for (int i = 0; i <= M - k; ++i) {
+            ta[i] = 0.5f * (ta[i] + ta[i + 1]);
+            tb[i] = 0.5f * (tb[i] + tb[i + 1]);
+            tw[i] = 0.5f * (tw[i] + tw[i + 1]);
+        }
+        upd(0, ta[0], tb[0], tw[0]);              // k-th point of the lower half
+        upd(1, ta[M - k], tb[M - k], tw[M - k]);  // of the upper half
+    }
+}
+
+template <int P, int Q>
+__device__ __forceinline__ bool subdiv_misses(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                              float lim) {
+    constexpr int NP = padded_points(P, Q);
+    auto coeff = [&](int k, float& a, float& b, float& w) {
+        const float x = __ldg(blk + k), y = __ldg(blk + NP + k), z = __ldg(blk + 2 * NP + k);
+        w = __ldg(blk + 3 * NP + k);
+        a = fmaf(r.n1x, x, fmaf(r.n1y, y, fmaf(r.n1z, z, pr.e1 * w)));
+        b = fmaf(r.n2x, x, fmaf(r.n2y, y, fmaf(r.n2z, z, pr.e2 * w)));
+    };
+    bool fu[2][4] = {{true, true, true, true}, {true, true, true, true}};
+#pragma unroll 1
+    for (int j = 0; j <= Q; ++j) {  // split every column at u = 1/2
+        float a[P + 1], b[P + 1], w[P + 1];
+#pragma unroll
+        for (int i = 0; i <= P; ++i) coeff(i * (Q + 1) + j, a[i], b[i], w[i]);
+        half_flags<P>(a, b, w, lim, fu);
+    }
+    if ((fu[0][0] | fu[0][1] | fu[0][2] | fu[0][3]) && (fu[1][0] | fu[1][1] | fu[1][2] | fu[1][3])) return true;
+    bool fv[2][4] = {{true, true, true, true}, {true, true, true, true}};
+#pragma unroll 1
+    for (int i = 0; i <= P; ++i) {  // split every row at v = 1/2
+        float a[Q + 1], b[Q + 1], w[Q + 1];
+#pragma unroll
+        for (int j = 0; j <= Q; ++j) coeff(i * (Q + 1) + j, a[j], b[j], w[j]);
+        half_flags<Q>(a, b, w, lim, fv);
+    }
+    return (fv[0][0] | fv[0][1] | fv[0][2] | fv[0][3]) && (fv[1][0] | fv[1][1] | fv[1][2] | fv[1][3]);
+}
+
 // One FP64 Newton step from a converged (u, v): evaluate in double, solve the
 // 2x2 system exactly in double, clamp, and move S to first order.
 template <int P, int Q>

@@ -10,11 +10,18 @@
 namespace nrt {
 namespace dev {
 
-constexpr int kEmitMax = 32;   // candidates one ray may emit in one round (K <= 24, plus one leaf)
+constexpr int kEmitMax = 16;   // candidates one ray may emit in one round (quota <= 8, plus one leaf)
+
+// A (ray, patch) work item carries its ray so that the per-class kernels read
+// items sequentially instead of gathering rays at random.
+struct __align__(16) WfItem {
+    float ox, oy, oz, dx, dy, dz;
+    int32_t ray, slot;
+};
 constexpr unsigned long long kNoHit = ~0ull;
 
-// Candidates per ray in round r: 1, 2, 4, 8, 16, then 24.
-__host__ __device__ constexpr int round_quota(int r) { return r >= 5 ? 24 : (1 << r); }
+// Candidates per ray in round r: 1, 2, 4, then 8.
+__host__ __device__ constexpr int round_quota(int r) { return r >= 3 ? 8 : (1 << r); }
 
 // Scratch of one wavefront launch over n rays (device pointers).
 struct WfBuffers {
@@ -26,10 +33,11 @@ struct WfBuffers {
     int32_t* counts;               // 4 ints: active count of the two lists, items of the round
     int32_t* emit_slot;            // n * kEmitMax: candidates emitted this round, by active position
     int32_t* emit_cnt;             // n
-    int2* items;                   // n * kEmitMax: (ray, slot) work items of a round, in rank order
+    WfItem* items;                 // n * kEmitMax: work items of a round, in rank order
     int32_t* hist;                 // n_slots + 1
     int32_t* cursor;               // n_slots + 1
     int32_t* offsets;              // n_slots + 1
+    int32_t* class_cursor;         // 64: next unclaimed item of each degree class
 };
 
 // Per-scene schedule data: patch ranks in (p, q, slot) order and the degree

@@ -11,6 +11,7 @@ from .lib import (  # noqa: F401
     Camera,
     Counters,
     IntersectOpts,
+    Mlp,
     NrtError,
     Scene,
     build_bvh_binary,

@@ -45,7 +45,8 @@ class HitsC(C.Structure):
 class IntersectOpts(C.Structure):
     _fields_ = [("init_mode", C.c_int), ("max_iter", C.c_int), ("eps", C.c_float), ("det_eps", C.c_float),
                 ("cond_fp64", C.c_float), ("fp64_final", C.c_int), ("hull_cull", C.c_int), ("schedule", C.c_int),
-                ("seed_offset", C.c_int), ("flat_threshold", C.c_float), ("cam_k", C.c_float)]
+                ("seed_offset", C.c_int), ("flat_threshold", C.c_float), ("cam_k", C.c_float),
+                ("learned_iters", C.c_int)]
 
     def replace(self, **kw) -> "IntersectOpts":
         o = IntersectOpts()
@@ -59,7 +60,7 @@ class IntersectOpts(C.Structure):
 
 
 _COUNTER_NAMES = ("rays", "box_tests", "patch_candidates", "patch_culled", "newton_solves", "newton_evals",
-                  "fp64_solves", "fp64_final_steps", "hits", "errors")
+                  "fp64_solves", "fp64_final_steps", "hits", "errors", "learned_solves", "learned_fallbacks")
 
 
 class Counters(C.Structure):
@@ -74,6 +75,11 @@ class Counters(C.Structure):
         d["kernel_launches"] = int(self.kernel_launches)
         d["rounds"] = int(self.rounds)
         return d
+
+
+class TrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint32)]
 
 
 class CameraC(C.Structure):
@@ -113,6 +119,21 @@ def lib():
         L.nrt_enable_counters.argtypes = [vp, C.c_int]
         L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
         L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
+        L.nrt_mlp_param_count.restype = C.c_size_t
+        L.nrt_mlp_create.argtypes = [C.c_int, C.c_uint32, C.POINTER(vp)]
+        L.nrt_mlp_destroy.argtypes = [vp]
+        L.nrt_mlp_get_params.argtypes = [vp, vp]
+        L.nrt_mlp_set_params.argtypes = [vp, vp]
+        L.nrt_mlp_forward.argtypes = [vp, vp, C.c_int64, vp, vp]
+        L.nrt_mlp_gradients.argtypes = [vp, vp, vp, C.c_int64, vp, C.POINTER(C.c_float), vp]
+        L.nrt_mlp_train.argtypes = [vp, vp, vp, C.c_int64, C.POINTER(TrainOpts), vp, vp]
+        L.nrt_mlp_save.argtypes = [vp, C.c_char_p]
+        L.nrt_mlp_load.argtypes = [C.c_char_p, C.c_int, C.POINTER(vp)]
+        L.nrt_scene_set_mlp.argtypes = [vp, vp]
+        L.nrt_collect_training_data.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts), vp, vp,
+                                                C.c_int64, C.POINTER(C.c_int64), vp]
+        L.nrt_intersect_noalloc.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts),
+                                            C.POINTER(HitsC), vp]
         _LIB = L
     return _LIB
 
@@ -252,6 +273,26 @@ class Scene:
         _check(lib().nrt_get_counters(self._h, C.byref(c), _stream_ptr(stream)))
         return c.as_dict()
 
+    def set_mlp(self, mlp: "Mlp"):
+        _check(lib().nrt_scene_set_mlp(self._h, mlp.handle))
+
+    def collect_training_data(self, rays, opts: IntersectOpts | None = None, capacity=None, stream=None):
+        """(features (m,12), targets (m,2)) CUDA tensors of converged plain-Newton solves."""
+        import torch
+
+        if opts is None:
+            opts = default_opts(schedule=SCHED_WAVEFRONT)
+        n = rays[0].numel()
+        cap = int(capacity if capacity is not None else 4 * n)
+        feat = torch.empty((cap, 12), dtype=torch.float32, device=rays[0].device)
+        targ = torch.empty((cap, 2), dtype=torch.float32, device=rays[0].device)
+        cnt = C.c_int64()
+        r = RaysC(*[C.c_void_p(a.data_ptr()) for a in rays])
+        _check(lib().nrt_collect_training_data(self._h, C.byref(r), n, C.byref(opts), C.c_void_p(feat.data_ptr()),
+                                               C.c_void_p(targ.data_ptr()), cap, C.byref(cnt), _stream_ptr(stream)))
+        m = min(cnt.value, cap)
+        return feat[:m], targ[:m], cnt.value
+
     def intersect(self, rays, opts: IntersectOpts | None = None, out=None, stream=None, geom=False, extra=True):
         """rays: 6 float32 CUDA tensors (ox, oy, oz, dx, dy, dz).  Returns a dict of CUDA tensors."""
         import torch
@@ -292,3 +333,73 @@ def camera_rays(cam, device="cuda", stream=None):
     r = RaysC(*[C.c_void_p(a.data_ptr()) for a in arrs])
     _check(lib().nrt_generate_camera_rays(C.byref(c), C.byref(r), _stream_ptr(stream)))
     return arrs
+
+
+class Mlp:
+    """The learned-initial-guess network (nrt_mlp_*)."""
+
+    N_PARAMS = 5122
+
+    def __init__(self, seed=0, device=0, handle=None):
+        self._h = C.c_void_p()
+        if handle is not None:
+            self._h = handle
+        else:
+            _check(lib().nrt_mlp_create(device, seed, C.byref(self._h)))
+
+    @classmethod
+    def load(cls, path, device=0):
+        h = C.c_void_p()
+        _check(lib().nrt_mlp_load(str(path).encode(), device, C.byref(h)))
+        return cls(handle=h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().nrt_mlp_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.N_PARAMS, np.float32)
+        _check(lib().nrt_mlp_get_params(self._h, out.ctypes.data))
+        return out
+
+    def set_params(self, theta):
+        theta = np.ascontiguousarray(theta, np.float32)
+        assert theta.size == self.N_PARAMS
+        _check(lib().nrt_mlp_set_params(self._h, theta.ctypes.data))
+
+    def forward(self, features, stream=None):
+        import torch
+
+        n = features.shape[0]
+        out = torch.empty((n, 2), dtype=torch.float32, device=features.device)
+        _check(lib().nrt_mlp_forward(self._h, C.c_void_p(features.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                     _stream_ptr(stream)))
+        return out
+
+    def gradients(self, features, targets, stream=None):
+        g = np.zeros(self.N_PARAMS, np.float32)
+        loss = C.c_float()
+        _check(lib().nrt_mlp_gradients(self._h, C.c_void_p(features.data_ptr()), C.c_void_p(targets.data_ptr()),
+                                       features.shape[0], g.ctypes.data, C.byref(loss), _stream_ptr(stream)))
+        return float(loss.value), g
+
+    def train(self, features, targets, epochs=20, batch=4096, lr=1e-3, seed=0, stream=None):
+        losses = np.zeros(epochs, np.float32)
+        o = TrainOpts(epochs, batch, lr, 0.0, 0.0, 0.0, seed)
+        _check(lib().nrt_mlp_train(self._h, C.c_void_p(features.data_ptr()), C.c_void_p(targets.data_ptr()),
+                                   features.shape[0], C.byref(o), losses.ctypes.data, _stream_ptr(stream)))
+        return losses
+
+    def save(self, path):
+        _check(lib().nrt_mlp_save(self._h, str(path).encode()))

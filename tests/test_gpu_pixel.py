@@ -94,10 +94,12 @@ def test_hull_cull_changes_nothing(nrt_gpu, name):
     scene = nrt_gpu.Scene(golden_surfaces(g))
     rays = gpu_rays(golden_rays(g))
     for base in [nrt_gpu.default_opts(), nrt_gpu.reference_opts()]:
-        a = to_numpy(scene.intersect(rays, base))
-        b = to_numpy(scene.intersect(rays, base.replace(hull_cull=1)))
-        for k in ("patch", "t", "u", "v", "iters"):
-            assert np.array_equal(a[k], b[k]), k
+        for sched in (nrt_gpu.SCHED_PIXEL, nrt_gpu.SCHED_WAVEFRONT):
+            a = to_numpy(scene.intersect(rays, base.replace(schedule=sched)))
+            for level in (1, 2):
+                b = to_numpy(scene.intersect(rays, base.replace(hull_cull=level, schedule=sched)))
+                for k in ("patch", "t", "u", "v", "iters"):
+                    assert np.array_equal(a[k], b[k]), (k, sched, level)
 
 
 def test_counters_and_empty_launch(nrt_gpu):
