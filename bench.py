@@ -283,6 +283,28 @@ def nrt_arm(args):
 
     ms_plain = timed(plain, max(1, args.steps // 2), 1) / max(1, args.steps // 2)
 
+    # the learned initial guess (committed model, or trained now), same workload
+    learned_block = None
+    try:
+        from nrt import learned
+
+        mlp, src = learned.load_or_train()
+        scene.set_mlp(mlp)
+        lopts = nrt.default_opts(hull_cull=2, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT,
+                                 init_mode=nrt.INIT_LEARNED, learned_iters=6)
+        scene.enable_counters(True)
+        step(lopts)
+        lc = scene.counters()
+        scene.enable_counters(False)
+        ms_learned = timed(lopts, max(1, args.steps // 2), 1) / max(1, args.steps // 2)
+        learned_block = {"value": round(world * n / (ms_learned * 1e-3) / 1e6, 3), "ms_per_step": round(ms_learned, 3),
+                         "model": src, "learned_iters": 6,
+                         "newton_evals_per_ray": round(lc["newton_evals"] / lc["rays"], 3),
+                         "learned_solves_per_ray": round(lc["learned_solves"] / lc["rays"], 3),
+                         "fallback_rate": round(lc["learned_fallbacks"] / max(1, lc["learned_solves"]), 4)}
+    except Exception as exc:  # reported, never silently replaced
+        learned_block = {"error": str(exc)[:200]}
+
     # end to end through the public API: pinned host rays -> device -> intersect -> hits back to host
     host_rays = [a.cpu().pin_memory() for a in rays]
     dev_rays = [torch.empty_like(a) for a in rays]
@@ -349,6 +371,7 @@ def nrt_arm(args):
                                "hit_rate": round(cnt["hits"] / cnt["rays"], 4),
                                "wavefront_rounds": cnt["rounds"], "kernels_per_step": cnt["kernel_launches"]},
                 "speedup_vs_plain_pixel": round(ms_plain / ms_step, 3),
+                "learned_init_wavefront": learned_block,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 24 * n,
                         "d2h_bytes_per_step": 16 * n},

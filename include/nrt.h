@@ -256,8 +256,8 @@ int nrt_mlp_load(const char* path, int device, nrt_mlp** out);
 /* Copy the network into the scene; enables NRT_INIT_LEARNED for it. */
 int nrt_scene_set_mlp(nrt_scene* scene, const nrt_mlp* mlp);
 /* Run the wavefront intersection with `opts` (which must use the midpoint
- * guess) and record, for every solve that converged, its 12 features and its
- * converged (u, v): training pairs for the network.  features: device
+ * guess) and record, for every solve, its 12 features and its converged
+ * (u, v), or (-1, -1) when it did not converge: training pairs for the network.  features: device
  * capacity x 12, targets: device capacity x 2; *count gets the number of pairs
  * found (it may exceed capacity; only capacity are written).  Synchronous. */
 int nrt_collect_training_data(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,

@@ -126,7 +126,17 @@ static dev::PatchFrame patch_frame(const float* P, int p, int q, double cx, doub
                            (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id};
     f.ox = (float)o[0]; f.oy = (float)o[1]; f.oz = (float)o[2];
     for (int k = 0; k < 9; ++k) f.m[k] = (float)inv[k];
-    f.flat = (float)(delta / std::max(scale, 1e-30));
+    double hmax = 0.0;  // half-thickness of the control net along the frame's h axis
+    for (int i = 0; i <= p; ++i)
+        for (int j = 0; j <= q; ++j) {
+            double X[3];
+            pt(i, j, X);
+            const double d3[3] = {X[0] - o[0], X[1] - o[1], X[2] - o[2]};
+            hmax = std::max(hmax, std::fabs(inv[6] * d3[0] + inv[7] * d3[1] + inv[8] * d3[2]));
+        }
+    f.slab = (float)std::max(hmax, 1e-6);
+    f.flat = (float)(hmax * std::sqrt(std::fabs(det)) / std::max(scale * scale, 1e-30));
+    (void)delta;
     f.lo[0] = (float)(b.lo[0] - cx); f.lo[1] = (float)(b.lo[1] - cy); f.lo[2] = (float)(b.lo[2] - cz);
     f.hi_x = (float)(b.hi[0] - cx); f.hi_y = (float)(b.hi[1] - cy); f.hi_z = (float)(b.hi[2] - cz);
     return f;

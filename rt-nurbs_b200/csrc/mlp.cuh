@@ -1,17 +1,18 @@
 // mlp.cuh -- the learned initial guess: features of a (ray, patch) pair and a
 // 12 -> 64 -> 64 -> 2 MLP (SiLU) on BF16 tensor cores with FP32 accumulation.
 //
-// Features (12), all dimensionless:
-//   0-2  ray entry into the patch's box, in the patch frame
-//   3-5  ray exit from the box, in the patch frame
-//   6-8  ray direction in the patch frame, normalised
+// Features (12), all dimensionless, in the patch frame:
+//   0-2  where the ray enters the patch's slab |h| <= H (clipped to its box)
+//   3-5  where it leaves the slab (same clipping); h is given as h/H
+//   6-8  ray direction, normalised
 //   9,10 p/7, q/7
-//   11   flatness: patchDelta (src/core/main.cpp:18-43) over the frame size
+//   11   slab half-thickness H over the frame size (a flatness measure, the
+//        role of patchDelta in src/core/main.cpp:18-43)
 // The patch frame maps a point X to (s, t, h) with X = o + s*A + t*B + h*N:
 // A and B are the mean u- and v-chords of the control net, N the unit normal
 // of A x B scaled by sqrt|A x B|, o the (0,0) corner, so that for a flat patch
-// (s, t) is close to the patch's (u, v).  The network maps the features to a
-// starting (u, v) for Newton.
+// (s, t) is close to the patch's (u, v) and the hit lies between the entry
+// and exit points.  The network maps the features to a starting (u, v).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -32,7 +33,7 @@ constexpr int kMlpLdIn = kMlpInPad + 8;   // padded row of inputs
 struct __align__(16) PatchFrame {
     float ox, oy, oz, flat;
     float m[9];
-    float pad0, pad1, pad2;
+    float slab, pad1, pad2;   // slab: half-thickness H of the control net in h
     float lo[3], hi_x;
     float hi_y, hi_z, pad3, pad4;
 };
@@ -63,33 +64,43 @@ __device__ __forceinline__ void features(const PatchFrame& f, int p, int q, cons
     const float t0x = (f.lo[0] - lox) * rdx, t1x = (f.hi_x - lox) * rdx;
     const float t0y = (f.lo[1] - loy) * rdy, t1y = (f.hi_y - loy) * rdy;
     const float t0z = (f.lo[2] - loz) * rdz, t1z = (f.hi_z - loz) * rdz;
-    float tin = fmaxf(fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))), 0.f);
-    float tout = fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
-    if (!(tout >= tin)) {  // grazing the box: use the point of closest approach to its centre
-        tin = fmaxf(-(lox * r.dx + loy * r.dy + loz * r.dz), 0.f);
-        tout = tin;
+    float bin = fmaxf(fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))), 0.f);
+    float bout = fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
+    if (!(bout >= bin)) {  // grazing the box: the point of closest approach to its centre
+        bin = fmaxf(-(lox * r.dx + loy * r.dy + loz * r.dz), 0.f);
+        bout = bin;
     }
-    const float ex = lox + tin * r.dx - f.ox, ey = loy + tin * r.dy - f.oy, ez = loz + tin * r.dz - f.oz;
-    const float xx = lox + tout * r.dx - f.ox, xy = loy + tout * r.dy - f.oy, xz = loz + tout * r.dz - f.oz;
-    x[0] = f.m[0] * ex + f.m[1] * ey + f.m[2] * ez;
-    x[1] = f.m[3] * ex + f.m[4] * ey + f.m[5] * ez;
-    x[2] = f.m[6] * ex + f.m[7] * ey + f.m[8] * ez;
-    x[3] = f.m[0] * xx + f.m[1] * xy + f.m[2] * xz;
-    x[4] = f.m[3] * xx + f.m[4] * xy + f.m[5] * xz;
-    x[5] = f.m[6] * xx + f.m[7] * xy + f.m[8] * xz;
-    const float dx = f.m[0] * r.dx + f.m[1] * r.dy + f.m[2] * r.dz;
-    const float dy = f.m[3] * r.dx + f.m[4] * r.dy + f.m[5] * r.dz;
-    const float dz = f.m[6] * r.dx + f.m[7] * r.dy + f.m[8] * r.dz;
-    const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
-    x[6] = dx * il;
-    x[7] = dy * il;
-    x[8] = dz * il;
+    // origin and direction in the frame
+    const float ax = lox - f.ox, ay = loy - f.oy, az = loz - f.oz;
+    const float os = f.m[0] * ax + f.m[1] * ay + f.m[2] * az;
+    const float ot = f.m[3] * ax + f.m[4] * ay + f.m[5] * az;
+    const float oh = f.m[6] * ax + f.m[7] * ay + f.m[8] * az;
+    const float ds = f.m[0] * r.dx + f.m[1] * r.dy + f.m[2] * r.dz;
+    const float dt = f.m[3] * r.dx + f.m[4] * r.dy + f.m[5] * r.dz;
+    const float dh = f.m[6] * r.dx + f.m[7] * r.dy + f.m[8] * r.dz;
+    // the slab |h| <= H, clipped to the box segment
+    float tin = bin, tout = bout;
+    if (fabsf(dh) > 1e-20f) {
+        const float ta = (-f.slab - oh) / dh, tb = (f.slab - oh) / dh;
+        const float sin_ = fmaxf(fminf(ta, tb), bin), sout = fminf(fmaxf(ta, tb), bout);
+        if (sout >= sin_) { tin = sin_; tout = sout; }
+    }
+    const float ih = 1.f / fmaxf(f.slab, 1e-30f);
+    x[0] = os + tin * ds;
+    x[1] = ot + tin * dt;
+    x[2] = (oh + tin * dh) * ih;
+    x[3] = os + tout * ds;
+    x[4] = ot + tout * dt;
+    x[5] = (oh + tout * dh) * ih;
+    const float il = rsqrtf(fmaxf(ds * ds + dt * dt + dh * dh, 1e-30f));
+    x[6] = ds * il;
+    x[7] = dt * il;
+    x[8] = dh * il;
     x[9] = (float)p * (1.f / 7.f);
     x[10] = (float)q * (1.f / 7.f);
     x[11] = f.flat;
-    // keep far-outside inputs bounded
 #pragma unroll
-    for (int k = 0; k < 6; ++k) x[k] = fminf(fmaxf(x[k], -8.f), 8.f);
+    for (int k = 0; k < 6; ++k) x[k] = fminf(fmaxf(x[k], -8.f), 8.f);  // keep far-outside inputs bounded
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -172,7 +183,7 @@ __device__ __forceinline__ void mlp_layer(const __nv_bfloat16 (*in)[LDA], const 
 }
 
 // Warp-synchronous inference: every lane of the warp passes its features and
-// receives its (u, v), clamped to [0, 1].  All 32 lanes must call it together.
+// receives the network's raw (u, v).  All 32 lanes must call it together.
 __device__ __forceinline__ void mlp_infer_warp(MlpSmem& s, int warp, int lane, const float (&x)[kMlpIn], float& u,
                                                float& v) {
 #pragma unroll
@@ -220,8 +231,8 @@ __device__ __forceinline__ void mlp_infer_warp(MlpSmem& s, int warp, int lane, c
     __syncwarp();
     mlp_layer<kMlpHidden, kMlpLd, kMlpOutPad, false>(h, s.w3t, s.b3, nullptr, s.y[warp], lane);
     __syncwarp();
-    u = fminf(fmaxf(s.y[warp][lane][0], 0.f), 1.f);
-    v = fminf(fmaxf(s.y[warp][lane][1], 0.f), 1.f);
+    u = s.y[warp][lane][0];
+    v = s.y[warp][lane][1];
     __syncwarp();
 }
 

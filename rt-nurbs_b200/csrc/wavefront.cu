@@ -222,16 +222,19 @@ __global__ void __launch_bounds__(1024) k_wf_scan(int m, WfBuffers wb) {
 // guess (init_mode 2) Newton first runs from the network's (u, v) for
 // learned_iters evaluations; if that does not converge it falls back to plain
 // Newton from (0.5, 0.5) with the full budget, which stays the judge of hits.
-// evals counts both attempts.
+// When the network's raw guess lies outside [-0.25, 1.25]^2 (it predicts no
+// root in the patch) the learned attempt is skipped and plain Newton runs
+// directly.  evals counts both attempts.
 template <int P, int Q>
 __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const RayFrame& r, const PatchRay& pr,
                                                 const float* __restrict__ blk, float lu, float lv, uint32_t seed,
                                                 const Opts& op, const NewtonOpts& nw, int& fell_back) {
     fell_back = 0;
-    if (op.init_mode == 2) {
+    const bool inside = lu >= -0.25f && lu <= 1.25f && lv >= -0.25f && lv <= 1.25f;
+    if (op.init_mode == 2 && inside) {
         NewtonOpts nl = nw;
         if (op.learned_iters > 0 && op.learned_iters < nw.max_iter) nl.max_iter = op.learned_iters;
-        const NewtonOut o = newton<P, Q>(blk, r, pr, lu, lv, seed, nl);
+        const NewtonOut o = newton<P, Q>(blk, r, pr, fminf(fmaxf(lu, 0.f), 1.f), fminf(fmaxf(lv, 0.f), 1.f), seed, nl);
         if (o.evals > 0) return o;
         fell_back = 1;
         NewtonOut f = newton<P, Q>(blk, r, pr, 0.5f, 0.5f, seed, nw);
@@ -239,6 +242,7 @@ __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const
         f.fp64_solves += o.fp64_solves;
         return f;
     }
+    if (op.init_mode == 2) fell_back = 2;  // gated off: plain Newton only
     float gu = 0.5f, gv = 0.5f;
     if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
     return newton<P, Q>(blk, r, pr, gu, gv, seed, nw);
@@ -336,18 +340,14 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
         float x[kMlpIn];
         float lu = 0.5f, lv = 0.5f;
         if (need_features) item_features(sc, k >= 0, k >= 0 ? it.slot : 0, h, C, r, pr, x);
-        if (op.init_mode == 2) {  // warp-synchronous: every lane takes part
-            mlp_infer_warp(*ms, warp, lane, x, lu, lv);
-            lu = fminf(fmaxf(lu, 0.f), 1.f);
-            lv = fminf(fmaxf(lv, 0.f), 1.f);
-        }
+        if (op.init_mode == 2) mlp_infer_warp(*ms, warp, lane, x, lu, lv);  // warp-synchronous
         if (k >= 0) {
             int fell = 0;
             const NewtonOut o = solve_item<P, Q>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
                                                  (uint32_t)it.ray + op.seed_offset, op, nw, fell);
             ++solves;
-            learned += op.init_mode == 2 ? 1 : 0;
-            fallbacks += (unsigned long long)fell;
+            learned += (op.init_mode == 2 && fell != 2) ? 1 : 0;
+            fallbacks += fell == 1 ? 1ull : 0ull;
             evals += (unsigned long long)(o.evals > 0 ? o.evals : -o.evals);
             f64 += (unsigned long long)o.fp64_solves;
             if (tests) atomicAdd(tests + it.ray, 1);
@@ -355,13 +355,13 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
                 const unsigned long long key = ((unsigned long long)__float_as_uint(o.t) << 32) | (unsigned)it.slot;
                 atomicMin(wb.best_key + it.ray, key);
             }
-            if (op.col_feat && o.evals > 0) {  // a training pair: features -> converged (u, v)
+            if (op.col_feat) {  // a training pair: features -> converged (u, v), or (-1, -1) if none
                 const unsigned long long at = atomicAdd(op.col_count, 1ull);
                 if ((long long)at < op.col_cap) {
 #pragma unroll
                     for (int q2 = 0; q2 < kMlpIn; ++q2) op.col_feat[at * kMlpIn + q2] = x[q2];
-                    op.col_targ[2 * at] = o.u;
-                    op.col_targ[2 * at + 1] = o.v;
+                    op.col_targ[2 * at] = o.evals > 0 ? o.u : -1.f;
+                    op.col_targ[2 * at + 1] = o.evals > 0 ? o.v : -1.f;
                 }
             }
         }
@@ -439,8 +439,6 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
             float x[kMlpIn];
             item_features(sc, valid, valid ? it.slot : 0, h, C, r, pr, x);
             mlp_infer_warp(*ms, warp, lane, x, lu, lv);
-            lu = fminf(fmaxf(lu, 0.f), 1.f);
-            lv = fminf(fmaxf(lv, 0.f), 1.f);
         }
         if (valid) {  // idle lanes wait at the __syncwarp below, so the next mma runs converged
         int fell = 0;
@@ -483,10 +481,23 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
     }
 }
 
-// Dynamic shared memory for the network, set once per kernel.
-template <class K>
-void allow_mlp_smem(K kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+// Dynamic shared memory for the network: the attribute is set once per kernel
+// (per process; every kernel of this file runs on devices of one architecture).
+template <int P, int Q>
+void allow_mlp_smem_newton() {
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(k_wf_newton<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+        done = true;
+    }
+}
+template <int P, int Q>
+void allow_mlp_smem_resolve() {
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(k_wf_resolve<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+        done = true;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -546,7 +557,7 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
             switch (pq) {
 #define NRT_CASE(P, Q) \
     case (P) | ((Q) << 4):                                                                              \
-        if (smem) allow_mlp_smem(k_wf_newton<P, Q>);                                                    \
+        if (smem) allow_mlp_smem_newton<P, Q>();                                                        \
         k_wf_newton<P, Q><<<grid, 256, smem, stream>>>(sc, rays, wb, c, rl, rh, op, out.tests, ctr);     \
         break;
                 NRT_FOR_EACH_DEGREE(NRT_CASE)
@@ -572,7 +583,7 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         switch (pq) {
 #define NRT_CASE(P, Q) \
     case (P) | ((Q) << 4):                                                                              \
-        if (smem) allow_mlp_smem(k_wf_resolve<P, Q>);                                                   \
+        if (smem) allow_mlp_smem_resolve<P, Q>();                                                       \
         k_wf_resolve<P, Q><<<grid, 256, smem, stream>>>(sc, wb, rl, rh, op, out, ctr);                   \
         break;
             NRT_FOR_EACH_DEGREE(NRT_CASE)

@@ -283,7 +283,7 @@ class Scene:
         if opts is None:
             opts = default_opts(schedule=SCHED_WAVEFRONT)
         n = rays[0].numel()
-        cap = int(capacity if capacity is not None else 4 * n)
+        cap = int(capacity if capacity is not None else 16 * n)
         feat = torch.empty((cap, 12), dtype=torch.float32, device=rays[0].device)
         targ = torch.empty((cap, 2), dtype=torch.float32, device=rays[0].device)
         cnt = C.c_int64()

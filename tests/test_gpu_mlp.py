@@ -86,11 +86,15 @@ def test_train_save_load(nrt_gpu, tmp_path):
     sc = scenes.surfaces_grid_scene(16, seed=21, width=256, height=144, spp=2)
     scene = nrt_gpu.Scene(sc.surfaces)
     rays = nrt_gpu.camera_rays(sc.camera)
-    feat, targ, total = scene.collect_training_data(rays, nrt_gpu.default_opts(schedule=nrt_gpu.SCHED_WAVEFRONT))
+    feat, targ, total = scene.collect_training_data(rays, nrt_gpu.default_opts(schedule=nrt_gpu.SCHED_WAVEFRONT),
+                                                    capacity=32 * rays[0].numel())
     assert feat.shape[0] == total > 5000
-    assert torch.isfinite(feat).all() and (targ >= 0).all() and (targ <= 1).all()
+    conv = targ[:, 0] >= 0  # converged solves; the others carry (-1, -1)
+    assert torch.isfinite(feat).all() and conv.sum() > 5000
+    assert ((targ[conv] >= 0) & (targ[conv] <= 1)).all() and (targ[~conv] == -1).all()
+    feat, targ = feat[conv].contiguous(), targ[conv].contiguous()
     mlp = nrt_gpu.Mlp(seed=5)
-    losses = mlp.train(feat, targ, epochs=6, batch=1024, lr=1e-3, seed=1)
+    losses = mlp.train(feat, targ, epochs=12, batch=256, lr=1e-3, seed=1)
     assert np.all(np.isfinite(losses))
     assert losses[-1] < losses[0] / 3, losses
     path = tmp_path / "init.mlp"
@@ -109,38 +113,37 @@ def test_train_save_load(nrt_gpu, tmp_path):
 
 
 def test_learned_init_gain_and_agreement(nrt_gpu, oracle_mod):
-    """Train on one seed, evaluate on an unseen one: hit agreement with the FP64
-    oracle (plain method) stays, and converged solves need fewer evaluations."""
-    from nrt import scenes
+    """Trained on height-field seeds 1..60, evaluated on the unseen seed 0: hit
+    agreement with the FP64 oracle (plain method) stays, and converged solves
+    need fewer Newton evaluations than from the midpoint guess."""
+    from nrt import learned, scenes
 
-    train = scenes.surfaces_grid_scene(16, seed=31, width=320, height=180, spp=2)
-    s_tr = nrt_gpu.Scene(train.surfaces)
-    feat, targ, _ = s_tr.collect_training_data(nrt_gpu.camera_rays(train.camera),
-                                               nrt_gpu.default_opts(schedule=nrt_gpu.SCHED_WAVEFRONT))
+    feat, targ = learned.collect(400_000, verbose=False,
+                                 which=[scenes.heightfield_scene(s, 256, 256, 1) for s in range(1, 61)])
     mlp = nrt_gpu.Mlp(seed=6)
-    mlp.train(feat, targ, epochs=10, batch=1024, lr=1e-3, seed=2)
-    test = scenes.surfaces_grid_scene(16, seed=32, width=320, height=180, spp=2)
+    mlp.train(feat, targ, epochs=20, batch=4096, lr=1e-3, seed=2)
+    test = scenes.heightfield_scene(0, 512, 512, 1)
     scene = nrt_gpu.Scene(test.surfaces)
     scene.set_mlp(mlp)
     rays = nrt_gpu.camera_rays(test.camera)
     W = nrt_gpu.SCHED_WAVEFRONT
     plain = nrt_gpu.default_opts(hull_cull=2, schedule=W)
-    learned = nrt_gpu.default_opts(hull_cull=2, schedule=W, init_mode=nrt_gpu.INIT_LEARNED, learned_iters=4)
+    learned_opts = nrt_gpu.default_opts(hull_cull=2, schedule=W, init_mode=nrt_gpu.INIT_LEARNED, learned_iters=6)
     scene.enable_counters(True)
     a = to_numpy(scene.intersect(rays, plain))
-    ca = scene.counters()
-    b = to_numpy(scene.intersect(rays, learned))
+    b = to_numpy(scene.intersect(rays, learned_opts))
     cb = scene.counters()
-    assert cb["learned_solves"] == cb["newton_solves"] > 0
+    assert 0 < cb["learned_solves"] <= cb["newton_solves"]
     P = oracle_mod.decompose_scene(test.surfaces, f64=False)
     P.cp64 = P.cp.astype(np.float64)
-    nb, lf, cnt, order, used = nrt_gpu.build_bvh_binary(nrt_gpu.patch_bounds(P.cp, P.off, P.deg), nrt_gpu.BVH_BINNED_SAH)
+    bvh = oracle_mod.build_bvh(oracle_mod.patch_boxes(P))
     r_np = oracle_mod.Rays(*[x.cpu().numpy() for x in rays])
-    ref = oracle_mod.intersect(P, oracle_mod.BinaryBVH(nb, lf, cnt, order, used), r_np, 0, 8, 1e-6, f64=True)
+    ref = oracle_mod.intersect(P, bvh, r_np, 0, 8, 1e-6, f64=True)
     st_plain = compare(a, ref.patch, ref.t, ref.u, ref.v)
     st_learn = compare(b, ref.patch, ref.t, ref.u, ref.v)
     assert st_plain["agree"] >= 0.9999, st_plain
     assert st_learn["agree"] >= 0.999, st_learn
-    hit = b["patch"] >= 0
-    assert b["iters"][hit].mean() < a["iters"][a["patch"] >= 0].mean(), (b["iters"][hit].mean(),
-                                                                        a["iters"][a["patch"] >= 0].mean())
+    assert st_learn["t_rel_max"] <= 1e-4, st_learn
+    plain_evals = a["iters"][a["patch"] >= 0].mean()
+    learned_evals = b["iters"][b["patch"] >= 0].mean()
+    assert learned_evals < 0.9 * plain_evals, (learned_evals, plain_evals)
