@@ -221,7 +221,7 @@ def nrt_arm(args):
         if world > 1:
             dist.barrier()
 
-    sc = scenes.mixed_degree_scene(1)
+    sc = scenes.mixed_degree_scene(1, spp=args.spp)
     sc.camera.seed = 1 + rank  # each rank its own samples
     t0 = time.perf_counter()
     scene = nrt.Scene(sc.surfaces)
@@ -229,7 +229,7 @@ def nrt_arm(args):
     rays = nrt.camera_rays(sc.camera)
     n = rays[0].numel()
     stream = torch.cuda.current_stream()
-    best = nrt.default_opts(hull_cull=2, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT)
+    best = nrt.default_opts(hull_cull=3, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT)
     plain = nrt.default_opts()
     out = {"patch": torch.empty(n, dtype=torch.int32, device="cuda"),
            "t": torch.empty(n, dtype=torch.float32, device="cuda"),
@@ -290,7 +290,7 @@ def nrt_arm(args):
 
         mlp, src = learned.load_or_train()
         scene.set_mlp(mlp)
-        lopts = nrt.default_opts(hull_cull=2, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT,
+        lopts = nrt.default_opts(hull_cull=3, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT,
                                  init_mode=nrt.INIT_LEARNED, learned_iters=6)
         scene.enable_counters(True)
         step(lopts)
@@ -391,9 +391,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="only launch the timed kernels (for ncu)")
     ap.add_argument("--profile-plain", action="store_true", help="with --profile: the plain per-pixel path")
+    ap.add_argument("--spp", type=int, default=4,
+                    help="samples per pixel (4 = the benchmark workload; fewer only for small profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and not args.profile:
         args.warmup = 3
+    if args.spp != 4 and not args.profile:
+        ap.error("--spp only applies to --profile runs; the benchmark workload is 4 spp")
     if args.impl == "reference":
         reference_arm(args)
     else:

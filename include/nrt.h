@@ -155,8 +155,13 @@ typedef struct {
     float det_eps;        /* |det J| below this takes the seeded pull step (1e-5) */
     float cond_fp64;      /* solve the 2x2 step in FP64 when cond(J) exceeds this; 0 = never */
     int fp64_final;       /* 1: one FP64 Newton step on the converged point */
-    int hull_cull;        /* 1: skip (ray, patch) tests whose control points all lie on
-                             one side of a ray plane by more than eps (result unchanged) */
+    int hull_cull;        /* skip (ray, patch) tests that provably cannot converge (results
+                             unchanged): 1 control points all on one side of a ray plane by
+                             more than eps; 2 also each half net split at u or v = 1/2;
+                             wavefront only: 3 as 2, after an oriented-box test of each
+                             patch during traversal; 4 the box test, then the exact 2D
+                             hull of the plane residuals and of both halves of the net
+                             split at u = 1/2, or at v = 1/2 */
     int schedule;         /* NRT_SCHED_PIXEL or NRT_SCHED_WAVEFRONT */
     int seed_offset;      /* added to the ray index to seed the singular-Jacobian pull */
     float flat_threshold; /* flat-skip in pixels (src/gpu/intersect.cu:104-123); 0 = off */

@@ -23,6 +23,7 @@ struct Scene {
     const float4* corners;   // per slot: four dehomogenised world-space corners q00, q10, q11, q01
     const float* delta;      // per slot: flatness (patchDelta) for flat-skip
     const PatchFrame* frames;  // per slot: frame of the learned guess's features
+    const float4* obb;       // per slot: oriented box of the control points, 4 float4 (see obb_misses)
     int n_slots;
 };
 

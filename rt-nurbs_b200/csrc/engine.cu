@@ -78,6 +78,78 @@ static float patch_delta(const float* P, int p, int q) {
     return d;
 }
 
+// Oriented bounding box of a patch's dehomogenised control points (their
+// convex hull holds the patch when every weight is positive): axes from the
+// principal directions of the points (cyclic Jacobi on the 3x3 covariance, in
+// double), extents from the points' projections.  Four float4 per slot:
+// (axis_k, half extent_k) for k = 0..2, then (centre, 0).  A patch with a
+// non-positive weight gets infinite extents, so that it is never culled.
+static void patch_obb(const float* P, int p, int q, float4 out[4]) {
+    const int n = (p + 1) * (q + 1);
+    std::vector<double> X(3 * (size_t)n);
+    bool pos = true;
+    double m[3] = {0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        const double w = P[4 * i + 3];
+        pos = pos && w > 0.0;
+        for (int k = 0; k < 3; ++k) {
+            X[3 * i + k] = w != 0.0 ? P[4 * i + k] / w : 0.0;
+            m[k] += X[3 * i + k] / n;
+        }
+    }
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) A[a][b] += (X[3 * i + a] - m[a]) * (X[3 * i + b] - m[b]);
+    for (int sweep = 0; sweep < 32; ++sweep) {
+        const double off = std::fabs(A[0][1]) + std::fabs(A[0][2]) + std::fabs(A[1][2]);
+        if (off <= 1e-300 + 1e-15 * (std::fabs(A[0][0]) + std::fabs(A[1][1]) + std::fabs(A[2][2]))) break;
+        for (int a = 0; a < 2; ++a)
+            for (int b = a + 1; b < 3; ++b) {
+                if (A[a][b] == 0.0) continue;
+                const double th = 0.5 * std::atan2(2.0 * A[a][b], A[b][b] - A[a][a]);
+                const double c = std::cos(th), s = std::sin(th);
+                for (int k = 0; k < 3; ++k) {  // A <- A J
+                    const double ka = A[k][a], kb = A[k][b];
+                    A[k][a] = c * ka - s * kb;
+                    A[k][b] = s * ka + c * kb;
+                }
+                for (int k = 0; k < 3; ++k) {  // A <- J^T A
+                    const double ak = A[a][k], bk = A[b][k];
+                    A[a][k] = c * ak - s * bk;
+                    A[b][k] = s * ak + c * bk;
+                }
+                for (int k = 0; k < 3; ++k) {  // V <- V J
+                    const double ka = V[k][a], kb = V[k][b];
+                    V[k][a] = c * ka - s * kb;
+                    V[k][b] = s * ka + c * kb;
+                }
+            }
+    }
+    double ctr[3] = {m[0], m[1], m[2]}, half[3];
+    for (int a = 0; a < 3; ++a) {
+        // round the axis to float first: the device projects with the stored axis
+        float ax[3] = {(float)V[0][a], (float)V[1][a], (float)V[2][a]};
+        double lo = 1e300, hi = -1e300;
+        for (int i = 0; i < n; ++i) {
+            const double t = ax[0] * (X[3 * i] - m[0]) + ax[1] * (X[3 * i + 1] - m[1]) + ax[2] * (X[3 * i + 2] - m[2]);
+            lo = std::min(lo, t);
+            hi = std::max(hi, t);
+        }
+        half[a] = 0.5 * (hi - lo);
+        for (int k = 0; k < 3; ++k) ctr[k] += ax[k] * 0.5 * (lo + hi);
+        out[a] = make_float4(ax[0], ax[1], ax[2], 0.f);
+    }
+    double cmax = 0.0;
+    for (int k = 0; k < 3; ++k) cmax = std::max(cmax, std::fabs(ctr[k]));
+    for (int a = 0; a < 3; ++a) {
+        // extents cover the float-rounded centre and axes
+        const double h = half[a] * (1.0 + 1e-6) + 4e-7 * cmax + 1e-30;
+        out[a].w = pos ? (float)(h * (1.0 + 1e-6)) : INFINITY;
+    }
+    out[3] = make_float4((float)ctr[0], (float)ctr[1], (float)ctr[2], 0.f);
+}
+
 // Frame of the learned guess's features (see mlp.cuh): origin at the (0,0)
 // corner, axes the mean u- and v-chords A, B of the control net and the
 // normal of A x B scaled by sqrt|A x B|; all in patch-local coordinates.
@@ -210,6 +282,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     std::vector<float4> corners(4 * (size_t)N);
     std::vector<float> delta(N);
     std::vector<dev::PatchFrame> frames(N);
+    std::vector<float4> obbs(4 * (size_t)N);
     std::vector<float> blocks;
     std::vector<int32_t> slot_patch(N);
     size_t total_floats = 0;
@@ -254,6 +327,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
         }
         delta[s] = patch_delta(P, p, q);
         frames[s] = patch_frame(P, p, q, cx, cy, cz, b, delta[s]);
+        patch_obb(P, p, q, &obbs[4 * (size_t)s]);
         info.degree_hist[p * 8 + q] += 1;
         off += 4 * (size_t)np;
     }
@@ -264,8 +338,9 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
                  sz_cen = align(N * sizeof(double4)), sz_cp = align(blocks.size() * sizeof(float)),
                  sz_cor = align(corners.size() * sizeof(float4)), sz_del = align(N * sizeof(float)),
                  sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long)),
-                 sz_rank = align(N * sizeof(int32_t)), sz_frm = align(N * sizeof(dev::PatchFrame));
-    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank + sz_frm;
+                 sz_rank = align(N * sizeof(int32_t)), sz_frm = align(N * sizeof(dev::PatchFrame)),
+                 sz_obb = align(obbs.size() * sizeof(float4));
+    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank + sz_frm + sz_obb;
     // wavefront plan: patches ranked by (p, q, slot); one class per degree pair present
     std::vector<int32_t> by_rank(N), rank_of(N);
     for (int s2 = 0; s2 < N; ++s2) by_rank[s2] = s2;
@@ -312,6 +387,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     at += sz_ctr;
     plan.rank_of = static_cast<const int32_t*>(put(rank_of.data(), N * sizeof(int32_t), sz_rank));
     sc->view.frames = static_cast<const dev::PatchFrame*>(put(frames.data(), N * sizeof(dev::PatchFrame), sz_frm));
+    sc->view.obb = static_cast<const float4*>(put(obbs.data(), obbs.size() * sizeof(float4), sz_obb));
     sc->plan = plan;
     cudaSetDevice(prev);
     if (e != cudaSuccess) {

@@ -193,40 +193,41 @@ __device__ __forceinline__ void mlp_infer_warp(MlpSmem& s, int warp, int lane, c
     __syncwarp();
     mlp_layer<kMlpInPad, kMlpLdIn, kMlpHidden, true>(s.x[warp], s.w1t, s.b1, s.h[warp], nullptr, lane);
     __syncwarp();
-    // layer 2 reads h and writes h: stage through the input tile's space is too small, so
-    // compute into registers first (mlp_layer writes only after all its reads of one row block)
+    // layer 2 reads h and writes h in place, one 16-row block at a time: a
+    // block's products only read its own rows, so its accumulators (32 floats
+    // per lane) are written back once every lane has read those rows.
     __nv_bfloat16 (*h)[kMlpLd] = s.h[warp];
     {
         const int g = lane >> 2, t = lane & 3;
-        float acc[2][8][4];
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
+        for (int mt = 0; mt < 2; ++mt) {
+            float acc[8][4];
+            const int r0 = mt * 16;
 #pragma unroll
             for (int nt = 0; nt < 8; ++nt) {
-                acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.f;
+                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
 #pragma unroll
                 for (int ks = 0; ks < 4; ++ks) {
-                    const int r0 = mt * 16, c0 = ks * 16;
+                    const int c0 = ks * 16;
                     const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&h[r0 + g][c0 + 2 * t]);
                     const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&h[r0 + g + 8][c0 + 2 * t]);
                     const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&h[r0 + g][c0 + 2 * t + 8]);
                     const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&h[r0 + g + 8][c0 + 2 * t + 8]);
                     const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&s.w2t[nt * 8 + g][c0 + 2 * t]);
                     const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&s.w2t[nt * 8 + g][c0 + 2 * t + 8]);
-                    mma_bf16(acc[mt][nt], a0, a1, a2, a3, b0, b1);
+                    mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
                 }
             }
-        __syncwarp();
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
+            __syncwarp();
 #pragma unroll
             for (int nt = 0; nt < 8; ++nt) {
-                const int col = nt * 8 + 2 * t, row = mt * 16 + g;
+                const int col = nt * 8 + 2 * t, row = r0 + g;
                 *reinterpret_cast<uint32_t*>(&h[row][col]) =
-                    pack_bf16(silu(acc[mt][nt][0] + s.b2[col]), silu(acc[mt][nt][1] + s.b2[col + 1]));
+                    pack_bf16(silu(acc[nt][0] + s.b2[col]), silu(acc[nt][1] + s.b2[col + 1]));
                 *reinterpret_cast<uint32_t*>(&h[row + 8][col]) =
-                    pack_bf16(silu(acc[mt][nt][2] + s.b2[col]), silu(acc[mt][nt][3] + s.b2[col + 1]));
+                    pack_bf16(silu(acc[nt][2] + s.b2[col]), silu(acc[nt][3] + s.b2[col + 1]));
             }
+        }
     }
     __syncwarp();
     mlp_layer<kMlpHidden, kMlpLd, kMlpOutPad, false>(h, s.w3t, s.b3, nullptr, s.y[warp], lane);

@@ -294,6 +294,195 @@ __device__ __forceinline__ bool subdiv_misses(const float* __restrict__ blk, con
     return (fv[0][0] | fv[0][1] | fv[0][2] | fv[0][3]) && (fv[1][0] | fv[1][1] | fv[1][2] | fv[1][3]);
 }
 
+// Exact ray-space hull test ("clip" cull).  With w > 0, (r1, r2)(u,v) =
+// (sum B_i a_i, sum B_i b_i) / sum B_i w_i, where (a_i, b_i) = (n1.P_i + e1 w_i,
+// n2.P_i + e2 w_i) are the homogeneous plane residuals of the control points.
+// If a unit direction d has d.(a_i, b_i) > M for every point, with
+// M = lim * max_i w_i, then d.(r1, r2) > lim everywhere on [0,1]^2, hence
+// |r1| + |r2| > lim >= eps and Newton cannot converge: the (ray, patch) test
+// is skipped without changing any result.  Such a d exists iff the origin lies
+// outside the convex hull of the points (up to the margin).
+//
+// Pass 1 keeps the arc of directions d with d.p > 0 for every point seen so
+// far: it starts as the half circle around the first point and each further
+// point either leaves it, trims one end to the point's perpendicular, or
+// empties it (origin inside the hull).  This is the exact 2D hull test in
+// O(points).  Pass 2 takes the arc's bisector and checks d.p_i > M |d| for
+// every point, so rounding in pass 1 can only cost a cull, never cause a
+// wrong one.  Subdividing the residual nets at u = 1/2 or v = 1/2 (de
+// Casteljau averages) tightens the hulls: a pair is also culled when both
+// halves' hulls miss the origin.
+struct Arc {
+    float rx, ry, lx, ly;  // clockwise and counter-clockwise ends of the arc of separating directions
+    int st;                // 0: no point yet, 1: arc non-empty, 2: empty (no separating direction)
+};
+
+__device__ __forceinline__ void arc_add(Arc& A, float px, float py) {
+    if (A.st == 1) {
+        const float sR = fmaf(A.rx, px, A.ry * py), sL = fmaf(A.lx, px, A.ly * py);
+        if (sR > 0.f) {
+            if (!(sL > 0.f)) { A.lx = -py; A.ly = px; }
+        } else if (sL > 0.f) {
+            A.rx = py; A.ry = -px;
+        } else {
+            A.st = 2;  // both ends outside the point's half circle (or NaN): no direction left
+        }
+    } else if (A.st == 0) {
+        A.rx = py; A.ry = -px; A.lx = -py; A.ly = px;
+        A.st = (px != 0.f || py != 0.f) ? 1 : 2;
+    }
+}
+
+// Bisector of the arc (unnormalised) and the margin it must clear: M * |d|.
+__device__ __forceinline__ bool arc_direction(const Arc& A, float M, float& dx, float& dy, float& need) {
+    if (A.st != 1) return false;
+    dx = A.rx + A.lx;
+    dy = A.ry + A.ly;
+    need = M * sqrtf(fmaf(dx, dx, dy * dy));
+    return dx != 0.f || dy != 0.f;
+}
+
+template <int P, int Q>
+__device__ __forceinline__ void residual_point(const float* __restrict__ blk, int k, const RayFrame& r,
+                                               const PatchRay& pr, float& a, float& b, float& w) {
+    constexpr int NP = padded_points(P, Q);
+    const float x = __ldg(blk + k), y = __ldg(blk + NP + k), z = __ldg(blk + 2 * NP + k);
+    w = __ldg(blk + 3 * NP + k);
+    a = fmaf(r.n1x, x, fmaf(r.n1y, y, fmaf(r.n1z, z, pr.e1 * w)));
+    b = fmaf(r.n2x, x, fmaf(r.n2y, y, fmaf(r.n2z, z, pr.e2 * w)));
+}
+
+// Depth 0: the whole net.  Returns true when the pair can be skipped; wmax
+// gets the largest weight (the margin's scale for the subdivided test).
+template <int P, int Q>
+__device__ __forceinline__ bool clip_whole(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                           float lim, float& wmax) {
+    constexpr int N = (P + 1) * (Q + 1);
+    Arc A;
+    A.st = 0;
+    wmax = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < N; ++k) {
+        float a, b, w;
+        residual_point<P, Q>(blk, k, r, pr, a, b, w);
+        wmax = fmaxf(wmax, w);
+        arc_add(A, a, b);
+    }
+    float dx, dy, need;
+    if (!arc_direction(A, lim * wmax, dx, dy, need)) return false;
+    bool sep = true;
+#pragma unroll 4
+    for (int k = 0; k < N; ++k) {
+        float a, b, w;
+        residual_point<P, Q>(blk, k, r, pr, a, b, w);
+        sep &= fmaf(dx, a, dy * b) > need;
+    }
+    return sep;
+}
+
+// Both halves of a degree-M polygon at 1/2 from one de Casteljau triangle:
+// lo holds the control values on t in [0, 1/2], hi those on [1/2, 1].
+template <int M>
+__device__ __forceinline__ void split_poly(const float (&c)[M + 1], float (&lo)[M + 1], float (&hi)[M + 1]) {
+    float t[M + 1];
+#pragma unroll
+    for (int i = 0; i <= M; ++i) t[i] = c[i];
+    lo[0] = t[0];
+    hi[M] = t[M];
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+#pragma unroll
+        for (int i = 0; i <= M - k; ++i) t[i] = 0.5f * (t[i] + t[i + 1]);
+        lo[k] = t[0];
+        hi[M - k] = t[M - k];
+    }
+}
+
+// Depth 1: the two halves of the net split at u = 1/2 (ALONG_U) or at
+// v = 1/2.  Every line of the net along the split direction is split on its
+// own, so the halves' points stream out one line at a time and no 2D net is
+// held in registers.  Returns true when both halves' hulls miss the origin.
+template <int P, int Q, bool ALONG_U>
+__device__ __forceinline__ bool clip_halves(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                            float M) {
+    constexpr int D = ALONG_U ? P : Q;           // degree along the split
+    constexpr int L = ALONG_U ? Q + 1 : P + 1;   // lines split
+    auto line = [&](int l, float (&la)[D + 1], float (&lb)[D + 1], float (&ua)[D + 1], float (&ub)[D + 1]) {
+        float a[D + 1], b[D + 1];
+#pragma unroll
+        for (int k = 0; k <= D; ++k) {
+            float w;
+            residual_point<P, Q>(blk, ALONG_U ? k * (Q + 1) + l : l * (Q + 1) + k, r, pr, a[k], b[k], w);
+        }
+        split_poly<D>(a, la, ua);
+        split_poly<D>(b, lb, ub);
+    };
+    Arc A0, A1;
+    A0.st = 0;
+    A1.st = 0;
+#pragma unroll 1
+    for (int l = 0; l < L; ++l) {
+        float la[D + 1], lb[D + 1], ua[D + 1], ub[D + 1];
+        line(l, la, lb, ua, ub);
+#pragma unroll
+        for (int k = 0; k <= D; ++k) {
+            arc_add(A0, la[k], lb[k]);
+            arc_add(A1, ua[k], ub[k]);
+        }
+        if (A0.st == 2 || A1.st == 2) return false;  // a half whose hull holds the origin
+    }
+    float d0x, d0y, n0, d1x, d1y, n1;
+    if (!arc_direction(A0, M, d0x, d0y, n0) || !arc_direction(A1, M, d1x, d1y, n1)) return false;
+    bool sep = true;
+#pragma unroll 1
+    for (int l = 0; l < L && sep; ++l) {
+        float la[D + 1], lb[D + 1], ua[D + 1], ub[D + 1];
+        line(l, la, lb, ua, ub);
+#pragma unroll
+        for (int k = 0; k <= D; ++k)
+            sep &= (fmaf(d0x, la[k], d0y * lb[k]) > n0) & (fmaf(d1x, ua[k], d1y * ub[k]) > n1);
+    }
+    return sep;
+}
+
+// The clip cull: the whole net, then its halves at u = 1/2, then at v = 1/2.
+template <int P, int Q>
+__device__ __forceinline__ bool clip_misses(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                            float lim) {
+    float wmax;
+    if (clip_whole<P, Q>(blk, r, pr, lim, wmax)) return true;
+    const float M = lim * wmax;
+    return clip_halves<P, Q, true>(blk, r, pr, M) || clip_halves<P, Q, false>(blk, r, pr, M);
+}
+
+// Oriented-box test of a (ray, patch) pair, before any work item is made.
+// The box holds the dehomogenised control points, hence the patch (w > 0).
+// It is widened by eps plus a rounding allowance for the FP32 projections, so
+// a ray that misses it cannot come within eps of the patch: Newton could not
+// converge there and the pair is dropped without changing any result.
+// obb: (axis_k, half extent_k) for k = 0..2, then (centre, 0).
+__device__ __forceinline__ bool obb_misses(const float4* __restrict__ obb, const RayFrame& r, float eps) {
+    const float4 a0 = __ldg(obb), a1 = __ldg(obb + 1), a2 = __ldg(obb + 2), c = __ldg(obb + 3);
+    const float ox = r.ox - c.x, oy = r.oy - c.y, oz = r.oz - c.z;
+    const float slack = eps + 1e-5f * (fabsf(ox) + fabsf(oy) + fabsf(oz) + a0.w + a1.w + a2.w);
+    float tn = -INFINITY, tf = INFINITY;
+    auto slab_k = [&](const float4 a) {
+        const float o = fmaf(a.x, ox, fmaf(a.y, oy, a.z * oz));
+        const float d = fmaf(a.x, r.dx, fmaf(a.y, r.dy, a.z * r.dz));
+        const float h = a.w + slack;
+        const float id = 1.f / d;
+        const float t0 = (-h - o) * id, t1 = (h - o) * id;
+        if (t0 == t0 && t1 == t1) {  // a NaN (d = 0 exactly on the boundary, or a NaN ray) constrains nothing
+            tn = fmaxf(tn, fminf(t0, t1));
+            tf = fminf(tf, fmaxf(t0, t1));
+        }
+    };
+    slab_k(a0);
+    slab_k(a1);
+    slab_k(a2);
+    return tf < tn;
+}
+
 // One FP64 Newton step from a converged (u, v): evaluate in double, solve the
 // 2x2 system exactly in double, clamp, and move S to first order.
 template <int P, int Q>

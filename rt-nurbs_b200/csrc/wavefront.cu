@@ -15,7 +15,7 @@
 //   k_wf_scan        exclusive scan of the per-rank counts.
 //   k_wf_scatter     work items (ray origin and direction, ray index, slot) in
 //                    rank order, ranks sorted by (p, q, slot).
-//   k_wf_newton<P,Q> one launch per degree class present in the scene: each
+//   k_wf_newton<P,Q,MODE> one launch per degree class present in the scene: each
 //                    warp takes 32 consecutive items (mostly one patch, so
 //                    control point loads broadcast), runs the exact hull tests
 //                    on them, compacts the survivors by ballot into a shared
@@ -24,7 +24,7 @@
 //                    (t bits << 32 | slot) with atomicMin.
 //
 // The resolve pass sorts the rays that hit by their winner's (p, q, slot) and
-// k_wf_resolve<P,Q> recomputes each winning solve (same code and inputs) with
+// k_wf_resolve<P,Q,LEARNED> recomputes each winning solve (same code and inputs) with
 // the FP64 final step and writes the hit record.  The closest hit is the
 // minimum over all candidates nearer than the best hit, so the order in which
 // candidates are solved does not change it.
@@ -140,6 +140,10 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
             const int first = leaf_first(ref), lc = leaf_count(ref);
             for (int s = first; s < first + lc; ++s) {
                 ++cands;
+                if (op.hull_cull >= 3 && obb_misses(sc.obb + 4 * s, r, op.nw.eps)) {
+                    ++culled;
+                    continue;
+                }
                 emit[emitted++] = s;  // quota <= 8 and a leaf holds <= 8: stays below kEmitMax
                 aggregated_add(wb.hist, rank_of[s]);
             }
@@ -186,13 +190,6 @@ __global__ void __launch_bounds__(256) k_wf_scatter(Rays rays, int round, int n_
     }
 }
 
-__device__ __forceinline__ void item_ray(const WfItem& it, RayFrame& r) {
-    r.ox = it.ox; r.oy = it.oy; r.oz = it.oz;
-    r.dx = it.dx; r.dy = it.dy; r.dz = it.dz;
-    ray_planes(r);
-}
-
-// Exclusive scan of hist[0..m) into offsets[0..m] (offsets[m] = total), and
 // cursor[] cleared; one block of 1024 threads.
 __global__ void __launch_bounds__(1024) k_wf_scan(int m, WfBuffers wb) {
     __shared__ int part[1024];
@@ -218,168 +215,6 @@ __global__ void __launch_bounds__(1024) k_wf_scan(int m, WfBuffers wb) {
     if (t == 1023) wb.offsets[m] = part[1023];
 }
 
-// One (ray, patch) solve with the options' initial guess.  With the learned
-// guess (init_mode 2) Newton first runs from the network's (u, v) for
-// learned_iters evaluations; if that does not converge it falls back to plain
-// Newton from (0.5, 0.5) with the full budget, which stays the judge of hits.
-// When the network's raw guess lies outside [-0.25, 1.25]^2 (it predicts no
-// root in the patch) the learned attempt is skipped and plain Newton runs
-// directly.  evals counts both attempts.
-template <int P, int Q>
-__device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const RayFrame& r, const PatchRay& pr,
-                                                const float* __restrict__ blk, float lu, float lv, uint32_t seed,
-                                                const Opts& op, const NewtonOpts& nw, int& fell_back) {
-    fell_back = 0;
-    const bool inside = lu >= -0.25f && lu <= 1.25f && lv >= -0.25f && lv <= 1.25f;
-    if (op.init_mode == 2 && inside) {
-        NewtonOpts nl = nw;
-        if (op.learned_iters > 0 && op.learned_iters < nw.max_iter) nl.max_iter = op.learned_iters;
-        const NewtonOut o = newton<P, Q>(blk, r, pr, fminf(fmaxf(lu, 0.f), 1.f), fminf(fmaxf(lv, 0.f), 1.f), seed, nl);
-        if (o.evals > 0) return o;
-        fell_back = 1;
-        NewtonOut f = newton<P, Q>(blk, r, pr, 0.5f, 0.5f, seed, nw);
-        f.evals = f.evals > 0 ? f.evals - o.evals : f.evals + o.evals;
-        f.fp64_solves += o.fp64_solves;
-        return f;
-    }
-    if (op.init_mode == 2) fell_back = 2;  // gated off: plain Newton only
-    float gu = 0.5f, gv = 0.5f;
-    if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
-    return newton<P, Q>(blk, r, pr, gu, gv, seed, nw);
-}
-
-// Features of the lane's item for the network (zeros for an idle lane).
-__device__ __forceinline__ void item_features(const Scene& sc, bool valid, int slot, const int4& h, const double4& C,
-                                              const RayFrame& r, const PatchRay& pr, float (&x)[kMlpIn]) {
-#pragma unroll
-    for (int k = 0; k < kMlpIn; ++k) x[k] = 0.f;
-    if (valid) features(sc.frames[slot], h.y & 15, (h.y >> 4) & 15, r, pr, C.x, C.y, C.z, x);
-}
-
-// Newton over the items of one degree class.  Each warp takes 32 items at a
-// time (chunks in a fixed stride), runs the hull tests on them (one lane per item;
-// the items of a warp mostly share a patch, so control point loads broadcast),
-// and queues the survivors in shared memory; Newton then runs on full warps of
-// survivors, so culled items do not leave lanes idle.
-template <int P, int Q>
-__global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
-                                                   int rank_hi, Opts op, int32_t* tests, unsigned long long* ctr) {
-    constexpr unsigned kFull = 0xffffffffu;
-    __shared__ int queue[8][64];
-    extern __shared__ __align__(16) unsigned char dyn_smem[];  // the network, when init_mode == 2
-    MlpSmem* ms = reinterpret_cast<MlpSmem*>(dyn_smem);
-    if (op.init_mode == 2) {
-        mlp_load(*ms, op.mlp);
-        __syncthreads();
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* qu = queue[warp];
-    const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
-    unsigned long long solves = 0, evals = 0, f64 = 0, culled = 0, hull_tests = 0, learned = 0, fallbacks = 0;
-    NewtonOpts nw = op.nw;
-    nw.fp64_final = 0;  // applied to the winner only, in k_wf_resolve
-    const bool need_features = op.init_mode == 2 || op.col_feat != nullptr;
-    const float cull_eps = op.nw.eps;
-    int qn = 0;
-    bool more = true;
-    // warps take 32-item chunks in a fixed stride (no shared cursor to contend on)
-    const int n_warps = gridDim.x * (blockDim.x >> 5);
-    int chunk = blockIdx.x * (blockDim.x >> 5) + warp;
-    while (true) {
-        while (more && qn < 32) {
-            const int base = begin + 32 * chunk;
-            chunk += n_warps;
-            if (base >= end) {
-                more = false;
-                break;
-            }
-            const int k = base + lane;
-            bool keep = false;
-            if (k < end) {
-                keep = true;
-                if (op.hull_cull) {
-                    const WfItem it = wb.items[k];
-                    const int4 h = sc.hdr[it.slot];
-                    if ((h.y >> 8) & kFlagPositiveWeights) {
-                        RayFrame r;
-                        item_ray(it, r);
-                        const double4 C = sc.centre[it.slot];
-                        const PatchRay pr = patch_ray(r, C.x, C.y, C.z);
-                        const float lim = cull_eps + 8e-6f * (float)C.w;
-                        ++hull_tests;
-                        if (hull_misses<P, Q>(sc.cp + h.x, r, pr, lim) ||
-                            (op.hull_cull >= 2 && subdiv_misses<P, Q>(sc.cp + h.x, r, pr, lim))) {
-                            keep = false;
-                            ++culled;
-                        }
-                    }
-                }
-            }
-            const unsigned m = __ballot_sync(kFull, keep);
-            if (keep) qu[qn + __popc(m & ((1u << lane) - 1))] = k;
-            qn += __popc(m);
-            __syncwarp();
-        }
-        if (qn == 0) break;
-        const int take = qn < 32 ? qn : 32;
-        const int k = lane < take ? qu[qn - take + lane] : -1;
-        qn -= take;
-        __syncwarp();
-        WfItem it;
-        RayFrame r;
-        int4 h = make_int4(0, 0, 0, 0);
-        double4 C = make_double4(0.0, 0.0, 0.0, 0.0);
-        PatchRay pr{};
-        if (k >= 0) {
-            it = wb.items[k];
-            item_ray(it, r);
-            h = sc.hdr[it.slot];
-            C = sc.centre[it.slot];
-            pr = patch_ray(r, C.x, C.y, C.z);
-        }
-        float x[kMlpIn];
-        float lu = 0.5f, lv = 0.5f;
-        if (need_features) item_features(sc, k >= 0, k >= 0 ? it.slot : 0, h, C, r, pr, x);
-        if (op.init_mode == 2) mlp_infer_warp(*ms, warp, lane, x, lu, lv);  // warp-synchronous
-        if (k >= 0) {
-            int fell = 0;
-            const NewtonOut o = solve_item<P, Q>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
-                                                 (uint32_t)it.ray + op.seed_offset, op, nw, fell);
-            ++solves;
-            learned += (op.init_mode == 2 && fell != 2) ? 1 : 0;
-            fallbacks += fell == 1 ? 1ull : 0ull;
-            evals += (unsigned long long)(o.evals > 0 ? o.evals : -o.evals);
-            f64 += (unsigned long long)o.fp64_solves;
-            if (tests) atomicAdd(tests + it.ray, 1);
-            if (o.evals > 0 && o.t > 0.f) {
-                const unsigned long long key = ((unsigned long long)__float_as_uint(o.t) << 32) | (unsigned)it.slot;
-                atomicMin(wb.best_key + it.ray, key);
-            }
-            if (op.col_feat) {  // a training pair: features -> converged (u, v), or (-1, -1) if none
-                const unsigned long long at = atomicAdd(op.col_count, 1ull);
-                if ((long long)at < op.col_cap) {
-#pragma unroll
-                    for (int q2 = 0; q2 < kMlpIn; ++q2) op.col_feat[at * kMlpIn + q2] = x[q2];
-                    op.col_targ[2 * at] = o.evals > 0 ? o.u : -1.f;
-                    op.col_targ[2 * at + 1] = o.evals > 0 ? o.v : -1.f;
-                }
-            }
-        }
-        __syncwarp();
-    }
-    if (ctr && op.counters) {
-        count_add(ctr, kSolves, solves);
-        count_add(ctr, kEvals, evals);
-        count_add(ctr, kFp64Solves, f64);
-        count_add(ctr, kCulled, culled);
-        count_add(ctr, kLearned, learned);
-        count_add(ctr, kFallbacks, fallbacks);
-        if (evals) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, evals);
-        if (hull_tests) atomicAdd(ctr + kHullByDegree + P * 8 + Q, hull_tests);
-    }
-}
-
-// Resolve, step 1: rays without a hit get their miss record; rays with one
 // emit their winning slot (counted per rank, as a round's candidates are).
 __global__ void __launch_bounds__(256) k_wf_resolve_emit(long long n, Opts op, WfBuffers wb, Hits out,
                                                          const int32_t* rank_of, unsigned long long* ctr) {
@@ -401,103 +236,6 @@ __global__ void __launch_bounds__(256) k_wf_resolve_emit(long long n, Opts op, W
     wb.emit_cnt[i] = 1;
     wb.emit_slot[(long long)i * kEmitMax] = s;
     aggregated_add(wb.hist, rank_of[s]);
-}
-
-// Resolve, step 2 (one launch per degree class): recompute the winning solve
-// (same code and inputs, so the same iterate) with the FP64 final step, and
-// write the hit record.
-template <int P, int Q>
-__global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int rank_lo, int rank_hi, Opts op,
-                                                    Hits out, unsigned long long* ctr) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    MlpSmem* ms = reinterpret_cast<MlpSmem*>(dyn_smem);
-    if (op.init_mode == 2) {
-        mlp_load(*ms, op.mlp);
-        __syncthreads();
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
-    unsigned long long f64f = 0, hits = 0, err = 0;
-    for (long long base = begin + ((long long)blockIdx.x * 8 + warp) * 32; base < end;
-         base += (long long)gridDim.x * 256) {
-        const long long k = base + lane;
-        const bool valid = k < end;
-        WfItem it;
-        RayFrame r;
-        int4 h = make_int4(0, 0, 0, 0);
-        double4 C = make_double4(0.0, 0.0, 0.0, 0.0);
-        PatchRay pr{};
-        if (valid) {
-            it = wb.items[k];
-            item_ray(it, r);
-            h = sc.hdr[it.slot];
-            C = sc.centre[it.slot];
-            pr = patch_ray(r, C.x, C.y, C.z);
-        }
-        float lu = 0.5f, lv = 0.5f;
-        if (op.init_mode == 2) {
-            float x[kMlpIn];
-            item_features(sc, valid, valid ? it.slot : 0, h, C, r, pr, x);
-            mlp_infer_warp(*ms, warp, lane, x, lu, lv);
-        }
-        if (valid) {  // idle lanes wait at the __syncwarp below, so the next mma runs converged
-        int fell = 0;
-        const NewtonOut o = solve_item<P, Q>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv, (uint32_t)it.ray + op.seed_offset,
-                                             op, op.nw, fell);
-        const long long i = it.ray;
-        if (o.evals > 0 && o.t > 0.f) {
-            ++hits;
-            f64f += (unsigned long long)o.fp64_final;
-            out.patch[i] = h.z;
-            out.t[i] = o.t;
-            out.u[i] = o.u;
-            out.v[i] = o.v;
-            if (out.iters) out.iters[i] = o.evals;
-            if (out.geom) {
-                float* g = out.geom + 9 * i;
-                g[0] = (float)(C.x + (double)o.sx); g[1] = (float)(C.y + (double)o.sy); g[2] = (float)(C.z + (double)o.sz);
-                g[3] = o.ux; g[4] = o.uy; g[5] = o.uz;
-                g[6] = o.vx; g[7] = o.vy; g[8] = o.vz;
-            }
-        } else {
-            if (o.evals <= 0) ++err;  // the recomputed winner must converge again
-            out.patch[i] = -1;
-            out.t[i] = -1.f;
-            out.u[i] = 0.f;
-            out.v[i] = 0.f;
-            if (out.iters) out.iters[i] = 0;
-            if (out.geom)
-                for (int a = 0; a < 9; ++a) out.geom[9 * i + a] = 0.f;
-        }
-        }
-        __syncwarp();
-    }
-    if (ctr) {
-        if (op.counters) {
-            count_add(ctr, kFp64Final, f64f);
-            count_add(ctr, kHits, hits);
-        }
-        if (err) atomicAdd(ctr + kErrors, err);
-    }
-}
-
-// Dynamic shared memory for the network: the attribute is set once per kernel
-// (per process; every kernel of this file runs on devices of one architecture).
-template <int P, int Q>
-void allow_mlp_smem_newton() {
-    static bool done = false;
-    if (!done) {
-        cudaFuncSetAttribute(k_wf_newton<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
-        done = true;
-    }
-}
-template <int P, int Q>
-void allow_mlp_smem_resolve() {
-    static bool done = false;
-    if (!done) {
-        cudaFuncSetAttribute(k_wf_resolve<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
-        done = true;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -530,13 +268,43 @@ WfBuffers wavefront_carve(void* base, long long n, int n_slots) {
     return b;
 }
 
+// The per-class kernels live in wf_solve.cu, one object per u-degree.
+static void wf_newton_class(int p, int q, const WfClassLaunch& L) {
+    switch (p) {
+        case 1: wf_newton_p1(q, L); break;
+        case 2: wf_newton_p2(q, L); break;
+        case 3: wf_newton_p3(q, L); break;
+        case 4: wf_newton_p4(q, L); break;
+        case 5: wf_newton_p5(q, L); break;
+        case 6: wf_newton_p6(q, L); break;
+        case 7: wf_newton_p7(q, L); break;
+        default: break;
+    }
+}
+
+static void wf_resolve_class(int p, int q, const WfClassLaunch& L) {
+    switch (p) {
+        case 1: wf_resolve_p1(q, L); break;
+        case 2: wf_resolve_p2(q, L); break;
+        case 3: wf_resolve_p3(q, L); break;
+        case 4: wf_resolve_p4(q, L); break;
+        case 5: wf_resolve_p5(q, L); break;
+        case 6: wf_resolve_p6(q, L); break;
+        case 7: wf_resolve_p7(q, L); break;
+        default: break;
+    }
+}
+
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds) {
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     int n_active = (int)n, cur = 0;
-    const size_t smem = op.init_mode == 2 ? sizeof(MlpSmem) : 0;
+    WfClassLaunch L{};
+    L.sc = &sc; L.rays = &rays; L.wb = &wb; L.op = &op; L.out = &out;
+    L.tests = out.tests; L.ctr = ctr; L.stream = stream;
+    L.mode = op.init_mode == 2 ? kWfLearned : (op.col_feat ? kWfCollect : kWfPlain);
     for (int round = 0; n_active > 0; ++round) {
         if (round > 4096) return cudaErrorUnknown;  // unreachable: every round pops at least one entry per ray
         e = cudaMemsetAsync(wb.hist, 0, sizeof(int) * plan.n_slots, stream);
@@ -552,18 +320,11 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         *launches += 3 + plan.n_classes;
         *rounds += 1;
         for (int c = 0; c < plan.n_classes; ++c) {
-            const int pq = plan.class_pq[c], rl = plan.class_rank[c], rh = plan.class_rank[c + 1];
-            const unsigned grid = plan.class_grid[c];
-            switch (pq) {
-#define NRT_CASE(P, Q) \
-    case (P) | ((Q) << 4):                                                                              \
-        if (smem) allow_mlp_smem_newton<P, Q>();                                                        \
-        k_wf_newton<P, Q><<<grid, 256, smem, stream>>>(sc, rays, wb, c, rl, rh, op, out.tests, ctr);     \
-        break;
-                NRT_FOR_EACH_DEGREE(NRT_CASE)
-#undef NRT_CASE
-                default: break;
-            }
+            L.cls = c;
+            L.rank_lo = plan.class_rank[c];
+            L.rank_hi = plan.class_rank[c + 1];
+            L.grid = plan.class_grid[c];
+            wf_newton_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
         }
         e = cudaMemcpyAsync(host_count, wb.counts + (1 - cur), sizeof(int), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -578,18 +339,11 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
     k_wf_scan<<<1, 1024, 0, stream>>>(plan.n_slots, wb);
     k_wf_scatter<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(rays, 0, (int)n, wb, cur, plan.rank_of);
     for (int c = 0; c < plan.n_classes; ++c) {
-        const int pq = plan.class_pq[c], rl = plan.class_rank[c], rh = plan.class_rank[c + 1];
-        const unsigned grid = plan.class_grid[c];
-        switch (pq) {
-#define NRT_CASE(P, Q) \
-    case (P) | ((Q) << 4):                                                                              \
-        if (smem) allow_mlp_smem_resolve<P, Q>();                                                       \
-        k_wf_resolve<P, Q><<<grid, 256, smem, stream>>>(sc, wb, rl, rh, op, out, ctr);                   \
-        break;
-            NRT_FOR_EACH_DEGREE(NRT_CASE)
-#undef NRT_CASE
-            default: break;
-        }
+        L.cls = c;
+        L.rank_lo = plan.class_rank[c];
+        L.rank_hi = plan.class_rank[c + 1];
+        L.grid = plan.class_grid[c];
+        wf_resolve_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
     }
     *launches += 3 + plan.n_classes;
     return cudaGetLastError();

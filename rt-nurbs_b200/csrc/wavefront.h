@@ -51,6 +51,42 @@ struct WfPlan {
     unsigned class_grid[64];  // blocks of 256 threads for the class's Newton kernel
 };
 
+// Kernel variants of a degree class: plain solve, plain solve that records
+// training pairs, solve from the network's guess.
+enum WfMode : int { kWfPlain = 0, kWfCollect = 1, kWfLearned = 2 };
+
+// Arguments of one per-class launch (k_wf_newton or k_wf_resolve).
+struct WfClassLaunch {
+    const Scene* sc;
+    const Rays* rays;
+    const WfBuffers* wb;
+    const Opts* op;
+    const Hits* out;
+    int32_t* tests;
+    unsigned long long* ctr;
+    cudaStream_t stream;
+    int mode;
+    int cls, rank_lo, rank_hi;
+    unsigned grid;
+};
+
+// Launchers of the per-class kernels for u-degree p (wf_solve.cu, one object
+// per p); q selects the v-degree.
+void wf_newton_p1(int q, const WfClassLaunch& L);
+void wf_newton_p2(int q, const WfClassLaunch& L);
+void wf_newton_p3(int q, const WfClassLaunch& L);
+void wf_newton_p4(int q, const WfClassLaunch& L);
+void wf_newton_p5(int q, const WfClassLaunch& L);
+void wf_newton_p6(int q, const WfClassLaunch& L);
+void wf_newton_p7(int q, const WfClassLaunch& L);
+void wf_resolve_p1(int q, const WfClassLaunch& L);
+void wf_resolve_p2(int q, const WfClassLaunch& L);
+void wf_resolve_p3(int q, const WfClassLaunch& L);
+void wf_resolve_p4(int q, const WfClassLaunch& L);
+void wf_resolve_p5(int q, const WfClassLaunch& L);
+void wf_resolve_p6(int q, const WfClassLaunch& L);
+void wf_resolve_p7(int q, const WfClassLaunch& L);
+
 // Bytes of scratch for n rays and a scene of n_slots patches.
 size_t wavefront_scratch_bytes(long long n, int n_slots);
 // Carve WfBuffers out of one block of at least wavefront_scratch_bytes(n, n_slots).

@@ -96,7 +96,7 @@ def test_hull_cull_changes_nothing(nrt_gpu, name):
     for base in [nrt_gpu.default_opts(), nrt_gpu.reference_opts()]:
         for sched in (nrt_gpu.SCHED_PIXEL, nrt_gpu.SCHED_WAVEFRONT):
             a = to_numpy(scene.intersect(rays, base.replace(schedule=sched)))
-            for level in (1, 2):
+            for level in (1, 2, 3, 4):
                 b = to_numpy(scene.intersect(rays, base.replace(hull_cull=level, schedule=sched)))
                 for k in ("patch", "t", "u", "v", "iters"):
                     assert np.array_equal(a[k], b[k]), (k, sched, level)

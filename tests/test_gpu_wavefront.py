@@ -105,3 +105,27 @@ def test_wavefront_chunks_and_overflow(nrt_gpu):
     sc = scenes.heightfield_scene(0, 64, 48)
     scene = nrt_gpu.Scene(sc.surfaces, wavefront_chunk=777)
     same_as_pixel(nrt_gpu, scene, nrt_gpu.camera_rays(sc.camera), nrt_gpu.default_opts(hull_cull=1, fp64_final=1))
+
+
+def test_clip_cull_changes_nothing(nrt_gpu):
+    """The oriented-box and exact hull culls (levels 3, 4) on 16 random mixed-degree surfaces, where
+    most (ray, patch) candidates that reach Newton have no root: bit-identical
+    hits to no cull at all, and more candidates culled than the levels below."""
+    from nrt import scenes
+
+    sc = scenes.surfaces_grid_scene(16, seed=5, width=320, height=180, spp=2)
+    scene = nrt_gpu.Scene(sc.surfaces)
+    rays = nrt_gpu.camera_rays(sc.camera)
+    W = nrt_gpu.SCHED_WAVEFRONT
+    culled = {}
+    base = to_numpy(scene.intersect(rays, nrt_gpu.default_opts(schedule=W)))
+    for level in (1, 2, 3, 4):
+        scene.enable_counters(True)
+        b = to_numpy(scene.intersect(rays, nrt_gpu.default_opts(schedule=W, hull_cull=level)))
+        c = scene.counters()
+        scene.enable_counters(False)
+        culled[level] = c["patch_culled"]
+        assert c["errors"] == 0
+        for k in ("patch", "t", "u", "v", "iters"):
+            assert np.array_equal(base[k], b[k]), (k, level)
+    assert culled[4] > culled[3] > culled[2] > culled[1] > 0, culled
