@@ -150,26 +150,55 @@ static void patch_obb(const float* P, int p, int q, float4 out[4]) {
     out[3] = make_float4((float)ctr[0], (float)ctr[1], (float)ctr[2], 0.f);
 }
 
-// Frame of the learned guess's features (see mlp.cuh): origin at the (0,0)
-// corner, axes the mean u- and v-chords A, B of the control net and the
-// normal of A x B scaled by sqrt|A x B|; all in patch-local coordinates.
-// Degenerate nets (collapsed edges) fall back to the box, normalised.
+// Frame of the learned guess's features (see mlp.cuh): the tangent frame of
+// the patch at (u, v) = (1/2, 1/2), in patch-local coordinates.  Axes A = dS/du,
+// B = dS/dv and the normal of A x B scaled by sqrt|A x B|; origin
+// S(1/2, 1/2) - A/2 - B/2, so that a point's frame coordinates (s, t) are its
+// (u, v) to first order (the iterate of one Newton step from the midpoint).
+// Rational evaluation in double from the weighted-homogeneous points.
+// Degenerate nets (collapsed tangents) fall back to the box, normalised.
 static dev::PatchFrame patch_frame(const float* P, int p, int q, double cx, double cy, double cz, const Box3& b,
                                    float delta) {
     auto pt = [&](int i, int j, double o[3]) {
         const float* c = P + 4 * (i * (q + 1) + j);
         o[0] = c[0] / (double)c[3] - cx; o[1] = c[1] / (double)c[3] - cy; o[2] = c[2] / (double)c[3] - cz;
     };
-    double A[3] = {0, 0, 0}, B[3] = {0, 0, 0}, o[3], t0[3], t1[3];
-    for (int j = 0; j <= q; ++j) {
-        pt(p, j, t1); pt(0, j, t0);
-        for (int k = 0; k < 3; ++k) A[k] += (t1[k] - t0[k]) / (q + 1);
+    // Bernstein values and derivatives at 1/2
+    auto bern = [](int n, double* B, double* dB) {
+        double c = 1.0;
+        for (int i = 0; i <= n; ++i) {
+            B[i] = c / std::ldexp(1.0, n);
+            c = c * (n - i) / (i + 1);
+        }
+        double cm = 1.0, Bm[8];
+        for (int i = 0; i < n; ++i) {
+            Bm[i] = cm / std::ldexp(1.0, n - 1);
+            cm = cm * (n - 1 - i) / (i + 1);
+        }
+        for (int i = 0; i <= n; ++i) dB[i] = n * ((i > 0 ? Bm[i - 1] : 0.0) - (i < n ? Bm[i] : 0.0));
+    };
+    double Bu[8], dBu[8], Bv[8], dBv[8];
+    bern(p, Bu, dBu);
+    bern(q, Bv, dBv);
+    double H[4] = {0, 0, 0, 0}, Hu[4] = {0, 0, 0, 0}, Hv[4] = {0, 0, 0, 0};
+    for (int i = 0; i <= p; ++i)
+        for (int j = 0; j <= q; ++j) {
+            const float* c = P + 4 * (i * (q + 1) + j);
+            const double w = c[3];
+            const double X[4] = {c[0] - w * cx, c[1] - w * cy, c[2] - w * cz, w};
+            for (int k = 0; k < 4; ++k) {
+                H[k] += Bu[i] * Bv[j] * X[k];
+                Hu[k] += dBu[i] * Bv[j] * X[k];
+                Hv[k] += Bu[i] * dBv[j] * X[k];
+            }
+        }
+    double A[3], B[3], o[3];
+    for (int k = 0; k < 3; ++k) {
+        const double S = H[k] / H[3];
+        A[k] = (Hu[k] - S * Hu[3]) / H[3];
+        B[k] = (Hv[k] - S * Hv[3]) / H[3];
+        o[k] = S - 0.5 * A[k] - 0.5 * B[k];
     }
-    for (int i = 0; i <= p; ++i) {
-        pt(i, q, t1); pt(i, 0, t0);
-        for (int k = 0; k < 3; ++k) B[k] += (t1[k] - t0[k]) / (p + 1);
-    }
-    pt(0, 0, o);
     const double N[3] = {A[1] * B[2] - A[2] * B[1], A[2] * B[0] - A[0] * B[2], A[0] * B[1] - A[1] * B[0]};
     const double nn = std::sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
     const double aa = A[0] * A[0] + A[1] * A[1] + A[2] * A[2], bb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];

@@ -9,10 +9,12 @@
 //   11   slab half-thickness H over the frame size (a flatness measure, the
 //        role of patchDelta in src/core/main.cpp:18-43)
 // The patch frame maps a point X to (s, t, h) with X = o + s*A + t*B + h*N:
-// A and B are the mean u- and v-chords of the control net, N the unit normal
-// of A x B scaled by sqrt|A x B|, o the (0,0) corner, so that for a flat patch
-// (s, t) is close to the patch's (u, v) and the hit lies between the entry
-// and exit points.  The network maps the features to a starting (u, v).
+// A and B are the tangents dS/du and dS/dv at the patch centre (u, v) =
+// (1/2, 1/2), N the normal of A x B scaled by sqrt|A x B|, and
+// o = S(1/2, 1/2) - A/2 - B/2, so that (s, t) equals (u, v) to first order
+// (where the ray crosses the tangent plane is one Newton step from the
+// midpoint) and the hit lies between the entry and exit points.  The network
+// maps the features to a starting (u, v).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -51,6 +53,15 @@ struct MlpParams {
 };
 
 __device__ __forceinline__ float silu(float x) { return x / (1.f + __expf(-x)); }
+// Inference: x * sigmoid(x) = h + h * tanh(h) with h = x / 2, on the hardware
+// tanh approximation (relative error about 2^-11, below the BF16 rounding of
+// the stored activation).
+__device__ __forceinline__ float silu_fast(float x) {
+    const float h = 0.5f * x;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+    return fmaf(h, t, h);
+}
 __device__ __forceinline__ float dsilu_f(float z) {
     const float s = 1.f / (1.f + __expf(-z));
     return s * (1.f + z * (1.f - s));
@@ -170,8 +181,8 @@ __device__ __forceinline__ void mlp_layer(const __nv_bfloat16 (*in)[LDA], const 
             const float v0 = d[0] + bias[col], v1 = d[1] + bias[col + 1];
             const float v2 = d[2] + bias[col], v3 = d[3] + bias[col + 1];
             if (ACT) {
-                *reinterpret_cast<uint32_t*>(&out[row][col]) = pack_bf16(silu(v0), silu(v1));
-                *reinterpret_cast<uint32_t*>(&out[row + 8][col]) = pack_bf16(silu(v2), silu(v3));
+                *reinterpret_cast<uint32_t*>(&out[row][col]) = pack_bf16(silu_fast(v0), silu_fast(v1));
+                *reinterpret_cast<uint32_t*>(&out[row + 8][col]) = pack_bf16(silu_fast(v2), silu_fast(v3));
             } else if (col == 0) {  // the two real outputs live in columns 0 and 1
                 yout[row][0] = v0;
                 yout[row][1] = v1;
@@ -223,9 +234,9 @@ __device__ __forceinline__ void mlp_infer_warp(MlpSmem& s, int warp, int lane, c
             for (int nt = 0; nt < 8; ++nt) {
                 const int col = nt * 8 + 2 * t, row = r0 + g;
                 *reinterpret_cast<uint32_t*>(&h[row][col]) =
-                    pack_bf16(silu(acc[nt][0] + s.b2[col]), silu(acc[nt][1] + s.b2[col + 1]));
+                    pack_bf16(silu_fast(acc[nt][0] + s.b2[col]), silu_fast(acc[nt][1] + s.b2[col + 1]));
                 *reinterpret_cast<uint32_t*>(&h[row + 8][col]) =
-                    pack_bf16(silu(acc[nt][2] + s.b2[col]), silu(acc[nt][3] + s.b2[col + 1]));
+                    pack_bf16(silu_fast(acc[nt][2] + s.b2[col]), silu_fast(acc[nt][3] + s.b2[col + 1]));
             }
         }
     }

@@ -75,11 +75,11 @@ template <int P, int Q, int MODE>
 __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
                                                    int rank_hi, Opts op, int32_t* tests, unsigned long long* ctr) {
     constexpr unsigned kFull = 0xffffffffu;
-    constexpr bool kLearned = MODE == kWfLearned, kFeatures = MODE != kWfPlain;
+    constexpr bool kUseNet = MODE == kWfLearned, kFeatures = MODE != kWfPlain;
     __shared__ int queue[8][64];
     extern __shared__ __align__(16) unsigned char dyn_smem[];  // the network, in the learned mode
     MlpSmem* ms = reinterpret_cast<MlpSmem*>(dyn_smem);
-    if constexpr (kLearned) {
+    if constexpr (kUseNet) {
         mlp_load(*ms, op.mlp);
         __syncthreads();
     }
@@ -153,13 +153,13 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
         float x[kMlpIn];
         float lu = 0.5f, lv = 0.5f;
         if constexpr (kFeatures) item_features(sc, k >= 0, k >= 0 ? it.slot : 0, h, C, r, pr, x);
-        if constexpr (kLearned) mlp_infer_warp(*ms, warp, lane, x, lu, lv);  // warp-synchronous
+        if constexpr (kUseNet) mlp_infer_warp(*ms, warp, lane, x, lu, lv);  // warp-synchronous
         if (k >= 0) {
             int fell = 0;
-            const NewtonOut o = solve_item<P, Q, kLearned>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
+            const NewtonOut o = solve_item<P, Q, kUseNet>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
                                                            (uint32_t)it.ray + op.seed_offset, op, nw, fell);
             ++solves;
-            learned += (kLearned && fell != 2) ? 1 : 0;
+            learned += (kUseNet && fell != 2) ? 1 : 0;
             fallbacks += fell == 1 ? 1ull : 0ull;
             evals += (unsigned long long)(o.evals > 0 ? o.evals : -o.evals);
             f64 += (unsigned long long)o.fp64_solves;
