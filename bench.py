@@ -260,13 +260,20 @@ def nrt_arm(args):
         return ms
 
     if args.profile:
-        # only the path's kernels, for ncu: warmup + steps launches of the timed configuration
+        # only the path's kernels, for ncu: warmup + steps launches of the timed configuration, with
+        # host-driven rounds (ncu does not profile the kernels inside the graph's device-side loop;
+        # the kernels are the same, only the traversal and scatter read their round from the host)
+        scene.set_tuning(graph=2)
         prof = plain if args.profile_plain else best
         for _ in range(args.warmup + args.steps):
             step(prof)
         torch.cuda.synchronize()
         scene.close()
         return
+    # launch shapes: the project's autotuner (cached per GPU / scene / options), outside the timed region
+    from nrt import autotune
+
+    tuning, tune_ms = autotune.tune(scene, rays, best, out=out)
     peaks = measured_peaks()
     sgemm = sgemm_peak_tflops(torch)
     # counted run (separate from timing) for algorithmic flops and iteration statistics
@@ -359,6 +366,7 @@ def nrt_arm(args):
                 "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": n, "patches": scene.info()["n_patches"],
                            "schedule": "wavefront", "opts": {k: (round(v, 9) if isinstance(v, float) else v)
                                                           for k, v in best.as_dict().items()},
+                           "tuning": tuning, "tuning_ms_per_call": None if tune_ms is None else round(tune_ms, 3),
                            "l2": "inputs (199 MB rays) and outputs (133 MB) exceed the 126 MB L2; no flush",
                            "scene_build_s": round(build_s, 3)},
                 "plain_pixel": {"value": round(world * n / (ms_plain * 1e-3) / 1e6, 3), "ms_per_step": round(ms_plain, 3),

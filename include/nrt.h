@@ -199,6 +199,30 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
 int nrt_intersect_noalloc(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
                           const nrt_hits* hits, void* stream);
 
+/* Launch shapes of the wavefront schedule, per scene: the autotuner's knobs
+ * (no reference counterpart; the reference has one fixed 16x16 launch,
+ * src/gpu/intersect.cu:205-217).  In nrt_scene_set_tuning a field <= 0 keeps
+ * its current value. */
+typedef struct {
+    int64_t step_blocks;     /* traversal kernel in the graph: persistent blocks of 128 threads that
+                                take 128 active rays at a time */
+    int64_t scatter_blocks;  /* work-item scatter in the graph: persistent blocks of 256 threads */
+    int32_t class_blocks;    /* blocks of 256 threads per degree-class Newton launch */
+    int32_t graph;           /* 1: rounds run inside one CUDA graph with a device-side loop (no host
+                                synchronisation); 2: host-driven rounds (one synchronisation each) */
+    int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 530 bytes per ray) */
+} nrt_wavefront_tuning;
+int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out);
+int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in);
+/* Autotuner: times nrt_intersect (wavefront) on these rays and buffers under
+ * candidate launch shapes, one knob at a time (coordinate descent over
+ * traversal and scatter grids, class-launch blocks and rays per pass; the
+ * graph/host-driven choice stays as set), and keeps the fastest on the scene.  *out gets it and
+ * *best_ms its time per call (CUDA events, `reps` calls after one untimed
+ * call).  Synchronous.  Results do not depend on the tuning. */
+int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                 const nrt_hits* hits, int reps, nrt_wavefront_tuning* out, float* best_ms, void* stream);
+
 /* Counters of the last nrt_intersect on this scene (synchronises the stream). */
 typedef struct {
     uint64_t rays, box_tests, patch_candidates, patch_culled, newton_solves, newton_evals, fp64_solves,

@@ -58,7 +58,7 @@ struct Opts {
 // Indices into the device counter block (nrt_counters order).
 enum Counter : int {
     kRays = 0, kBoxTests, kCandidates, kCulled, kSolves, kEvals, kFp64Solves, kFp64Final, kHits, kErrors, kLearned,
-    kFallbacks, kNumCounters
+    kFallbacks, kRoundsDone, kNumCounters
 };
 // Followed by 64 per-degree evaluation counts and 64 per-degree hull-test counts.
 constexpr int kEvalsByDegree = kNumCounters, kHullByDegree = kNumCounters + 64, kCounterWords = kNumCounters + 128;

@@ -271,6 +271,14 @@ struct nrt_scene {
     int32_t* host_count = nullptr;  // pinned word for the per-round active count
     long long last_launches = 0, last_rounds = 0;  // of the last nrt_intersect
     void* mlp_blob = nullptr;    // the scene's copy of the learned guess's network
+    // The wavefront as a CUDA graph: the last one built, the arguments it was
+    // built for (pointers, sizes, options, launch shapes) and its pass count.
+    cudaGraphExec_t wf_graph = nullptr;
+    std::vector<unsigned char> wf_graph_key;
+    long long wf_graph_passes = 0;
+    bool last_graph = false;     // the last nrt_intersect ran the graph (rounds counted on the device)
+    dev::WfTuning tuning{};
+    bool use_graph = true;       // false: host-driven rounds
 };
 
 
@@ -588,6 +596,7 @@ int nrt_scene_destroy(nrt_scene* scene) {
     }
     if (scene->host_count) cudaFreeHost(scene->host_count);
     if (scene->mlp_blob) cudaFree(scene->mlp_blob);
+    if (scene->wf_graph) cudaGraphExecDestroy(scene->wf_graph);
     cudaSetDevice(prev);
     delete scene;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFree(scene)");
@@ -655,6 +664,7 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     if (prev != scene->device) NRT_CUDA(cudaSetDevice(scene->device), "cudaSetDevice");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     dev::Opts d;
+    std::memset(&d, 0, sizeof(d));  // padding too: the options are part of the graph's key
     to_dev_opts(o, d, scene->counters_on);
     if (scene->mlp_blob) d.mlp = blob_params(scene->mlp_blob);
     if (scene->counters_on)
@@ -665,6 +675,7 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     cudaError_t e = cudaSuccess;
     scene->last_launches = 0;
     scene->last_rounds = 0;
+    scene->last_graph = false;
     if (o.schedule == NRT_SCHED_PIXEL) {
         e = dev::launch_intersect_pixel(scene->view, r, (long long)n, d, h, scene->counters, st);
         scene->last_launches = 1;
@@ -694,19 +705,159 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
             }
         }
         const dev::WfBuffers wb = dev::wavefront_carve(scene->wf_ws, scene->wf_rays, scene->plan.n_slots);
-        for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
-            const long long m = std::min(chunk, (long long)n - at);
-            dev::Rays rc{r.ox + at, r.oy + at, r.oz + at, r.dx + at, r.dy + at, r.dz + at};
-            dev::Hits hc{h.patch + at, h.t + at, h.u + at, h.v + at, h.iters ? h.iters + at : nullptr,
-                         h.tests ? h.tests + at : nullptr, h.geom ? h.geom + 9 * at : nullptr};
-            dev::Opts dc = d;
-            dc.seed_offset = d.seed_offset + (uint32_t)at;  // seeds follow the global ray index
-            e = dev::launch_wavefront(scene->view, scene->plan, rc, m, dc, hc, wb, scene->host_count,
-                                      scene->counters, st, &scene->last_launches, &scene->last_rounds);
+        // the graph is rebuilt when any of its arguments changed
+        std::vector<unsigned char> key;
+        auto add = [&](const void* p, size_t b) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            key.insert(key.end(), c, c + b);
+        };
+        const long long nn = n;
+        add(&r, sizeof(r));
+        add(&h, sizeof(h));
+        add(&nn, sizeof(nn));
+        add(&chunk, sizeof(chunk));
+        add(&scene->wf_ws, sizeof(scene->wf_ws));
+        add(&scene->wf_rays, sizeof(scene->wf_rays));  // the scratch layout follows from it
+        add(&d, sizeof(d));
+        add(&scene->tuning, sizeof(scene->tuning));
+        if (!scene->use_graph) {
+            for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
+                const long long m = std::min(chunk, (long long)n - at);
+                dev::Rays rc{r.ox + at, r.oy + at, r.oz + at, r.dx + at, r.dy + at, r.dz + at};
+                dev::Hits hc{h.patch + at, h.t + at, h.u + at, h.v + at, h.iters ? h.iters + at : nullptr,
+                             h.tests ? h.tests + at : nullptr, h.geom ? h.geom + 9 * at : nullptr};
+                dev::Opts dc = d;
+                dc.seed_offset = d.seed_offset + (uint32_t)at;  // seeds follow the global ray index
+                e = dev::launch_wavefront(scene->view, scene->plan, rc, m, dc, hc, wb, scene->host_count,
+                                          scene->counters, st, &scene->last_launches, &scene->last_rounds);
+            }
+            if (prev != scene->device) cudaSetDevice(prev);
+            if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
+            return NRT_OK;
         }
+        if (!scene->wf_graph || key != scene->wf_graph_key) {
+            if (scene->wf_graph) cudaGraphExecDestroy(scene->wf_graph);
+            scene->wf_graph = nullptr;
+            scene->wf_graph_key.clear();
+            e = dev::build_wavefront_graph(scene->view, scene->plan, r, (long long)n, chunk, d, h, wb,
+                                           scene->counters, scene->tuning, &scene->wf_graph,
+                                           &scene->wf_graph_passes);
+            if (e == cudaSuccess) scene->wf_graph_key = std::move(key);
+        }
+        if (e == cudaSuccess) e = cudaGraphLaunch(scene->wf_graph, st);
+        scene->last_graph = true;
     }
     if (prev != scene->device) cudaSetDevice(prev);
     if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
+    return NRT_OK;
+}
+
+int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out) {
+    if (!scene || !out) return fail(NRT_ERR_INVALID, "null argument");
+    out->step_blocks = scene->tuning.step_blocks;
+    out->scatter_blocks = scene->tuning.scatter_blocks;
+    out->class_blocks = scene->tuning.class_blocks > 0 ? scene->tuning.class_blocks : (int32_t)scene->plan.class_grid[0];
+    out->graph = scene->use_graph ? 1 : 2;
+    out->chunk = scene->wf_chunk;
+    return NRT_OK;
+}
+
+int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in) {
+    if (!scene || !in) return fail(NRT_ERR_INVALID, "null argument");
+    if (in->step_blocks > (1LL << 24) || in->scatter_blocks > (1LL << 24) || in->class_blocks > (1 << 24))
+        return fail(NRT_ERR_INVALID, "block counts above 2^24");
+    if (in->graph > 2) return fail(NRT_ERR_INVALID, "graph must be 1 (graph) or 2 (host-driven)");
+    if (in->chunk > (1LL << 30)) return fail(NRT_ERR_INVALID, "chunk above 2^30 rays");
+    if (in->step_blocks > 0) scene->tuning.step_blocks = in->step_blocks;
+    if (in->scatter_blocks > 0) scene->tuning.scatter_blocks = in->scatter_blocks;
+    if (in->class_blocks > 0) scene->tuning.class_blocks = in->class_blocks;
+    if (in->graph > 0) scene->use_graph = in->graph == 1;
+    if (in->chunk > 0) scene->wf_chunk = in->chunk;  // the scratch is re-carved on the next call
+    return NRT_OK;
+}
+
+int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
+                 const nrt_hits* hits, int reps, nrt_wavefront_tuning* out, float* best_ms, void* stream) {
+    if (!scene || !rays || !opts || !hits || !out) return fail(NRT_ERR_INVALID, "null argument");
+    if (n <= 0) return fail(NRT_ERR_INVALID, "autotuning needs rays");
+    if (reps < 1 || reps > 1000) return fail(NRT_ERR_INVALID, "reps %d outside 1..1000", reps);
+    nrt_intersect_opts o = *opts;
+    o.schedule = NRT_SCHED_WAVEFRONT;
+    const int was_on = scene->counters_on;
+    scene->counters_on = 0;  // time the plain launches
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != scene->device) NRT_CUDA(cudaSetDevice(scene->device), "cudaSetDevice");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    int status = ce == cudaSuccess ? NRT_OK : cuda_fail(ce, "cudaEventCreate");
+    auto trial = [&](const nrt_wavefront_tuning& t, float& ms) -> int {
+        int rc = nrt_scene_set_tuning(scene, &t);
+        if (rc == NRT_OK) rc = nrt_intersect(scene, rays, n, &o, hits, stream);  // builds the graph, if any
+        if (rc != NRT_OK) return rc;
+        cudaError_t e = cudaEventRecord(e0, st);
+        for (int k = 0; k < reps && rc == NRT_OK; ++k) rc = nrt_intersect(scene, rays, n, &o, hits, stream);
+        if (rc != NRT_OK) return rc;
+        if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) return cuda_fail(e, "autotune timing");
+        ms /= (float)reps;
+        return NRT_OK;
+    };
+    nrt_wavefront_tuning best{};
+    if (status == NRT_OK) status = nrt_scene_get_tuning(scene, &best);
+    float best_t = 0.f;
+    if (status == NRT_OK) status = trial(best, best_t);
+    const long long rays_blocks = (n + 127) / 128;
+    const int64_t steps[] = {148 * 4, 148 * 8, 148 * 16, 148 * 64};
+    const int64_t scats[] = {148 * 4, 148 * 8, 148 * 16, 148 * 64};
+    const int32_t classes[] = {148 * 2, 148 * 4, 148 * 8, 148 * 16};
+    const int64_t chunks[] = {1LL << 21, 1LL << 22, 1LL << 23};
+    for (int pass = 0; pass < 2 && status == NRT_OK; ++pass) {
+        auto knob = [&](auto&& values, int count, auto&& set) {
+            for (int k = 0; k < count && status == NRT_OK; ++k) {
+                nrt_wavefront_tuning t = best;
+                if (!set(t, values[k])) continue;
+                float ms = 0.f;
+                status = trial(t, ms);
+                if (status == NRT_OK && ms < best_t) {
+                    best_t = ms;
+                    best = t;
+                }
+            }
+        };
+        knob(steps, 4, [&](nrt_wavefront_tuning& t, int64_t v) {
+            if (v == t.step_blocks || (v > rays_blocks && t.step_blocks >= rays_blocks)) return false;
+            t.step_blocks = v;
+            return true;
+        });
+        knob(scats, 4, [&](nrt_wavefront_tuning& t, int64_t v) {
+            if (v == t.scatter_blocks || (v > rays_blocks && t.scatter_blocks >= rays_blocks)) return false;
+            t.scatter_blocks = v;
+            return true;
+        });
+        knob(classes, 4, [&](nrt_wavefront_tuning& t, int32_t v) {
+            if (v == t.class_blocks) return false;
+            t.class_blocks = v;
+            return true;
+        });
+        knob(chunks, 3, [&](nrt_wavefront_tuning& t, int64_t v) {
+            if (v == t.chunk || (v > n && t.chunk >= n)) return false;
+            t.chunk = v;
+            return true;
+        });
+    }
+    if (status == NRT_OK) status = nrt_scene_set_tuning(scene, &best);
+    scene->counters_on = was_on;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (prev != scene->device) cudaSetDevice(prev);
+    if (status != NRT_OK) return status;
+    *out = best;
+    if (best_ms) *best_ms = best_t;
     return NRT_OK;
 }
 
@@ -734,8 +885,14 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
     out->errors = h[dev::kErrors];
     out->learned_solves = h[dev::kLearned];
     out->learned_fallbacks = h[dev::kFallbacks];
-    out->kernel_launches = (uint64_t)scene->last_launches;
-    out->rounds = (uint64_t)scene->last_rounds;
+    if (scene->last_graph) {  // rounds counted on the device; kernels per pass and per round are fixed
+        const uint64_t per_pass = 4 + (uint64_t)scene->plan.n_classes, per_round = 4 + (uint64_t)scene->plan.n_classes;
+        out->rounds = h[dev::kRoundsDone];
+        out->kernel_launches = (uint64_t)scene->wf_graph_passes * per_pass + out->rounds * per_round;
+    } else {
+        out->kernel_launches = (uint64_t)scene->last_launches;
+        out->rounds = (uint64_t)scene->last_rounds;
+    }
     for (int k = 0; k < 64; ++k) {
         out->evals_by_degree[k] = h[dev::kEvalsByDegree + k];
         out->hull_tests_by_degree[k] = h[dev::kHullByDegree + k];
@@ -817,6 +974,7 @@ int noalloc_views(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
 void noalloc_record(nrt_scene* scene, long long launches, long long rounds) {
     scene->last_launches = launches;
     scene->last_rounds = rounds;
+    scene->last_graph = false;
 }
 
 }  // namespace nrt

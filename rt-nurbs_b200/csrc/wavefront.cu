@@ -34,6 +34,8 @@
 #include "kernels.h"
 #include "wavefront.h"
 
+#include <algorithm>
+
 namespace nrt {
 namespace dev {
 
@@ -63,12 +65,16 @@ __device__ __forceinline__ int aggregated_add(int* hist, int key) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long n, int round, int n_active,
-                                                 int quota, Opts op, WfBuffers wb, int cur, int32_t* tests,
-                                                 unsigned long long* ctr, const int32_t* rank_of) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n_active) return;
-    const long long i = round == 0 ? (long long)j : (long long)wb.active[cur][j];
+struct StepTally {
+    unsigned long long boxes, cands, culled, err;
+};
+
+// One active ray j (ray index i) for one round: resume its saved stack, emit
+// up to `quota` leaf patches, save the stack, and queue the ray for the next
+// round if its stack is not empty.
+__device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long long n, int round, int j, long long i,
+                                         int quota, const Opts& op, const WfBuffers& wb, int cur, int32_t* tests,
+                                         const int32_t* rank_of, StepTally& c) {
     RayFrame r;
     load_ray(rays, i, r);
     const float rdx = __frcp_rn(r.dx), rdy = __frcp_rn(r.dy), rdz = __frcp_rn(r.dz);
@@ -93,7 +99,6 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
     }
     int32_t* emit = wb.emit_slot + (long long)j * kEmitMax;
     int emitted = 0;
-    unsigned long long boxes = 0, cands = 0, culled = 0, err = 0;
     while (sp > 0 && emitted < quota) {
         --sp;
         const int ref = st[sp];
@@ -114,7 +119,7 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 if (CH[q] < 0 && CN[q] == 0) continue;
-                ++boxes;
+                ++c.boxes;
                 const float t = slab(LX[q], LY[q], LZ[q], HX[q], HY[q], HZ[q], r, rdx, rdy, rdz);
                 if (t < best) {
                     tt[k] = t;
@@ -133,15 +138,15 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
                     stt[sp] = tt[a];
                     ++sp;
                 } else {
-                    ++err;  // stack overflow: the subtree is dropped and the error counted
+                    ++c.err;  // stack overflow: the subtree is dropped and the error counted
                 }
             }
         } else {
             const int first = leaf_first(ref), lc = leaf_count(ref);
             for (int s = first; s < first + lc; ++s) {
-                ++cands;
+                ++c.cands;
                 if (op.hull_cull >= 3 && obb_misses(sc.obb + 4 * s, r, op.nw.eps)) {
-                    ++culled;
+                    ++c.culled;
                     continue;
                 }
                 emit[emitted++] = s;  // quota <= 8 and a leaf holds <= 8: stays below kEmitMax
@@ -159,22 +164,64 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
         const int at = aggregated_add(wb.counts + (1 - cur), 0);
         wb.active[1 - cur][at] = (int)i;
     }
-    if (ctr) {
-        if (op.counters) {
-            if (round == 0) count_add(ctr, kRays, 1);
-            count_add(ctr, kBoxTests, boxes);
-            count_add(ctr, kCandidates, cands);
-            count_add(ctr, kCulled, culled);
-        }
-        if (err) atomicAdd(ctr + kErrors, err);
-    }
 }
 
-__global__ void __launch_bounds__(256) k_wf_scatter(Rays rays, int round, int n_active, WfBuffers wb, int cur,
-                                                    const int32_t* rank_of) {
+__device__ __forceinline__ void step_count(unsigned long long* ctr, const Opts& op, unsigned long long rays,
+                                           const StepTally& c) {
+    if (!ctr) return;
+    if (op.counters) {
+        count_add(ctr, kRays, rays);
+        count_add(ctr, kBoxTests, c.boxes);
+        count_add(ctr, kCandidates, c.cands);
+        count_add(ctr, kCulled, c.culled);
+    }
+    if (c.err) atomicAdd(ctr + kErrors, c.err);
+}
+
+// Host-driven round: the host passes the round, its active count and list.
+__global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long n, int round, int n_active,
+                                                 int quota, Opts op, WfBuffers wb, int cur, int32_t* tests,
+                                                 unsigned long long* ctr, const int32_t* rank_of) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n_active) return;
-    const int i = round == 0 ? j : wb.active[cur][j];
+    StepTally c{};
+    if (j < n_active)
+        step_ray(sc, rays, n, round, j, round == 0 ? (long long)j : (long long)wb.active[cur][j], quota, op, wb, cur,
+                 tests, rank_of, c);
+    step_count(ctr, op, (round == 0 && j < n_active) ? 1ull : 0ull, c);
+}
+
+// Device-driven round (inside the CUDA graph's loop): the round number is
+// counts[2], the active list and count follow from it.  Persistent blocks
+// take 128 rays at a time from the round's work counter (counts[4]), so the
+// grid can be sized to the GPU and a round with few active rays costs no
+// empty blocks.
+__global__ void __launch_bounds__(128) k_wf_step_dev(Scene sc, Rays rays, long long n, Opts op, WfBuffers wb,
+                                                     int32_t* tests, unsigned long long* ctr, const int32_t* rank_of) {
+    __shared__ int s_base;
+    const int round = wb.counts[2], cur = round & 1;
+    const int n_active = round == 0 ? (int)n : wb.counts[cur];
+    const int quota = round_quota(round);
+    StepTally c{};
+    unsigned long long seen = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_base = atomicAdd(wb.counts + 4, (int)blockDim.x);
+        __syncthreads();
+        const int base = s_base;
+        __syncthreads();
+        if (base >= n_active) break;
+        const int j = base + threadIdx.x;
+        if (j < n_active) {
+            step_ray(sc, rays, n, round, j, round == 0 ? (long long)j : (long long)wb.active[cur][j], quota, op, wb,
+                     cur, tests, rank_of, c);
+            ++seen;
+        }
+    }
+    step_count(ctr, op, round == 0 ? seen : 0ull, c);
+}
+
+// Work items of active ray j (ray index i), placed in rank order.
+__device__ __forceinline__ void scatter_ray(const Rays& rays, int j, int i, const WfBuffers& wb,
+                                            const int32_t* rank_of) {
     const int m = wb.emit_cnt[j];
     if (m == 0) return;
     WfItem it;
@@ -188,6 +235,57 @@ __global__ void __launch_bounds__(256) k_wf_scatter(Rays rays, int round, int n_
         it.slot = s;
         wb.items[pos] = it;
     }
+}
+
+__global__ void __launch_bounds__(256) k_wf_scatter(Rays rays, int round, int n_active, WfBuffers wb, int cur,
+                                                    const int32_t* rank_of) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_active) return;
+    scatter_ray(rays, j, round == 0 ? j : wb.active[cur][j], wb, rank_of);
+}
+
+// Persistent as k_wf_step_dev, on its own work counter (counts[5]).
+__global__ void __launch_bounds__(256) k_wf_scatter_dev(Rays rays, long long n, WfBuffers wb,
+                                                        const int32_t* rank_of) {
+    __shared__ int s_base;
+    const int round = wb.counts[2], cur = round & 1;
+    const int n_active = round == 0 ? (int)n : wb.counts[cur];
+    for (;;) {
+        if (threadIdx.x == 0) s_base = atomicAdd(wb.counts + 5, (int)blockDim.x);
+        __syncthreads();
+        const int base = s_base;
+        __syncthreads();
+        if (base >= n_active) break;
+        const int j = base + threadIdx.x;
+        if (j < n_active) scatter_ray(rays, j, round == 0 ? j : wb.active[cur][j], wb, rank_of);
+    }
+}
+
+// Graph loop bookkeeping.  init: round 0, empty lists and work counters, and
+// a clear histogram.  round_end: clear what the next round counts into (its
+// active list's count and the work counters; k_wf_scan already cleared the
+// histogram), advance the round and continue the loop while rays are left.
+__global__ void __launch_bounds__(256) k_wf_init(WfBuffers wb, int n_slots) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_slots; k += gridDim.x * blockDim.x) wb.hist[k] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < 8) wb.counts[threadIdx.x] = 0;
+}
+
+constexpr int kMaxRounds = 4096;  // every round pops at least one stack entry per active ray
+
+__global__ void k_wf_round_end(WfBuffers wb, cudaGraphConditionalHandle loop, unsigned long long* ctr) {
+    if (threadIdx.x != 0) return;
+    const int round = wb.counts[2], cur = round & 1;
+    const int next = wb.counts[1 - cur];
+    const bool more = next > 0 && round + 1 < kMaxRounds;
+    if (ctr) {
+        atomicAdd(ctr + kRoundsDone, 1ull);
+        if (next > 0 && !more) atomicAdd(ctr + kErrors, 1ull);
+    }
+    wb.counts[cur] = 0;  // the next round queues its survivors into this list
+    wb.counts[4] = 0;
+    wb.counts[5] = 0;
+    wb.counts[2] = round + 1;
+    cudaGraphSetConditional(loop, more ? 1u : 0u);
 }
 
 // cursor[] cleared; one block of 1024 threads.
@@ -208,9 +306,11 @@ __global__ void __launch_bounds__(1024) k_wf_scan(int m, WfBuffers wb) {
     }
     int run = part[t] - s;
     for (int k = a; k < b; ++k) {
+        const int hk = wb.hist[k];
         wb.offsets[k] = run;
-        run += wb.hist[k];
+        run += hk;
         wb.cursor[k] = 0;
+        wb.hist[k] = 0;  // cleared for the next round
     }
     if (t == 1023) wb.offsets[m] = part[1023];
 }
@@ -242,7 +342,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve_emit(long long n, Opts op, W
 size_t wavefront_scratch_bytes(long long n, int n_slots) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t N = (size_t)n, S = (size_t)n_slots + 1;
-    return 2 * al(N * kStack * 4) + al(N * 4) + al(N * 8) + 2 * al(N * 4) + al(16) + al(N * kEmitMax * 4) +
+    return 2 * al(N * kStack * 4) + al(N * 4) + al(N * 8) + 2 * al(N * 4) + al(32) + al(N * kEmitMax * 4) +
            al(N * 4) + al(N * kEmitMax * sizeof(WfItem)) + 3 * al(S * 4) + al(64 * 4);
 }
 
@@ -257,7 +357,7 @@ WfBuffers wavefront_carve(void* base, long long n, int n_slots) {
     b.best_key = reinterpret_cast<unsigned long long*>(p); p += al(N * 8);
     b.active[0] = reinterpret_cast<int32_t*>(p); p += al(N * 4);
     b.active[1] = reinterpret_cast<int32_t*>(p); p += al(N * 4);
-    b.counts = reinterpret_cast<int32_t*>(p); p += al(16);
+    b.counts = reinterpret_cast<int32_t*>(p); p += al(32);
     b.emit_slot = reinterpret_cast<int32_t*>(p); p += al(N * kEmitMax * 4);
     b.emit_cnt = reinterpret_cast<int32_t*>(p); p += al(N * 4);
     b.items = reinterpret_cast<WfItem*>(p); p += al(N * kEmitMax * sizeof(WfItem));
@@ -309,7 +409,6 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         if (round > 4096) return cudaErrorUnknown;  // unreachable: every round pops at least one entry per ray
         e = cudaMemsetAsync(wb.hist, 0, sizeof(int) * plan.n_slots, stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(wb.counts + (1 - cur), 0, sizeof(int), stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(wb.class_cursor, 0, sizeof(int) * 64, stream);
         if (e != cudaSuccess) return e;
         k_wf_step<<<(unsigned)((n_active + 127) / 128), 128, 0, stream>>>(sc, rays, n, round, n_active,
                                                                          round_quota(round), op, wb, cur, out.tests,
@@ -347,6 +446,121 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
     }
     *launches += 3 + plan.n_classes;
     return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace nrt
+
+namespace nrt {
+namespace dev {
+
+namespace {
+
+// Records the launches of `fill` on stream cs into a new graph.
+template <class F>
+cudaError_t capture(cudaStream_t cs, cudaGraph_t* g, F&& fill) {
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return e;
+    fill();
+    const cudaError_t le = cudaGetLastError();
+    e = cudaStreamEndCapture(cs, g);
+    return le != cudaSuccess ? le : e;
+}
+
+}  // namespace
+
+cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n,
+                                  long long chunk, const Opts& op, const Hits& out, const WfBuffers& wb,
+                                  unsigned long long* ctr, const WfTuning& tu, cudaGraphExec_t* exec,
+                                  long long* passes) {
+    *exec = nullptr;
+    *passes = 0;
+    if (n <= 0 || chunk <= 0) return cudaErrorInvalidValue;
+    cudaGraph_t g = nullptr;
+    cudaStream_t cs = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    cudaGraphNode_t prev = nullptr;
+    const int mode = op.init_mode == 2 ? kWfLearned : (op.col_feat ? kWfCollect : kWfPlain);
+    for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
+        const long long m = std::min(chunk, n - at);
+        const Rays rc{rays.ox + at, rays.oy + at, rays.oz + at, rays.dx + at, rays.dy + at, rays.dz + at};
+        const Hits hc{out.patch + at, out.t + at, out.u + at, out.v + at, out.iters ? out.iters + at : nullptr,
+                      out.tests ? out.tests + at : nullptr, out.geom ? out.geom + 9 * at : nullptr};
+        Opts oc = op;
+        oc.seed_offset = op.seed_offset + (uint32_t)at;  // seeds follow the global ray index
+        WfClassLaunch L{};
+        L.sc = &sc; L.rays = &rc; L.wb = &wb; L.op = &oc; L.out = &hc;
+        L.tests = hc.tests; L.ctr = ctr; L.stream = cs; L.mode = mode;
+        // the pass's set-up
+        cudaGraph_t pre = nullptr;
+        e = capture(cs, &pre, [&] {
+            k_wf_init<<<std::max(1u, std::min(148u * 2, (unsigned)((plan.n_slots + 255) / 256))), 256, 0, cs>>>(
+                wb, plan.n_slots);
+        });
+        cudaGraphNode_t n_pre = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_pre, g, prev ? &prev : nullptr, prev ? 1 : 0, pre);
+        if (pre) cudaGraphDestroy(pre);
+        // the rounds: a while node whose body is one round
+        cudaGraphConditionalHandle loop = 0;
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t n_loop = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&n_loop, g, &n_pre, 1, &cp);
+        if (e == cudaSuccess) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+            if (e == cudaSuccess) {
+                const unsigned step_grid = (unsigned)std::max(1LL, std::min<long long>((m + 127) / 128, tu.step_blocks));
+                const unsigned scat_grid = (unsigned)std::max(1LL, std::min<long long>((m + 255) / 256, tu.scatter_blocks));
+                k_wf_step_dev<<<step_grid, 128, 0, cs>>>(sc, rc, m, oc, wb, hc.tests, ctr, plan.rank_of);
+                k_wf_scan<<<1, 1024, 0, cs>>>(plan.n_slots, wb);
+                k_wf_scatter_dev<<<scat_grid, 256, 0, cs>>>(rc, m, wb, plan.rank_of);
+                for (int c = 0; c < plan.n_classes; ++c) {
+                    L.cls = c;
+                    L.rank_lo = plan.class_rank[c];
+                    L.rank_hi = plan.class_rank[c + 1];
+                    L.grid = tu.class_blocks > 0 ? (unsigned)tu.class_blocks : plan.class_grid[c];
+                    wf_newton_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
+                }
+                k_wf_round_end<<<1, 32, 0, cs>>>(wb, loop, ctr);
+                const cudaError_t le = cudaGetLastError();
+                cudaGraph_t got = nullptr;
+                e = cudaStreamEndCapture(cs, &got);
+                if (e == cudaSuccess) e = le;
+            }
+        }
+        // resolve: hit rays sorted by their winner's (p, q, slot), one kernel per class
+        cudaGraph_t post = nullptr;
+        if (e == cudaSuccess)
+            e = capture(cs, &post, [&] {
+                cudaMemsetAsync(wb.hist, 0, sizeof(int) * plan.n_slots, cs);
+                k_wf_resolve_emit<<<(unsigned)((m + 255) / 256), 256, 0, cs>>>(m, oc, wb, hc, plan.rank_of, ctr);
+                k_wf_scan<<<1, 1024, 0, cs>>>(plan.n_slots, wb);
+                k_wf_scatter<<<(unsigned)((m + 255) / 256), 256, 0, cs>>>(rc, 0, (int)m, wb, 0, plan.rank_of);
+                for (int c = 0; c < plan.n_classes; ++c) {
+                    L.cls = c;
+                    L.rank_lo = plan.class_rank[c];
+                    L.rank_hi = plan.class_rank[c + 1];
+                    L.grid = plan.class_grid[c];
+                    wf_resolve_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
+                }
+            });
+        cudaGraphNode_t n_post = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_post, g, &n_loop, 1, post);
+        if (post) cudaGraphDestroy(post);
+        prev = n_post;
+        ++*passes;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    if (e != cudaSuccess) *exec = nullptr;
+    if (g) cudaGraphDestroy(g);
+    if (cs) cudaStreamDestroy(cs);
+    return e;
 }
 
 }  // namespace dev

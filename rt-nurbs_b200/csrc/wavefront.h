@@ -30,7 +30,8 @@ struct WfBuffers {
     int32_t* stack_sp;             // n
     unsigned long long* best_key;  // n: (t bits << 32) | slot of the nearest hit so far
     int32_t* active[2];            // n each: ray indices still traversing (ping-pong)
-    int32_t* counts;               // 4 ints: active count of the two lists, items of the round
+    int32_t* counts;               // 8 ints: active counts of the two lists, round (graph), -, work
+                                   // counters of the persistent step and scatter kernels (graph)
     int32_t* emit_slot;            // n * kEmitMax: candidates emitted this round, by active position
     int32_t* emit_cnt;             // n
     WfItem* items;                 // n * kEmitMax: work items of a round, in rank order
@@ -91,6 +92,25 @@ void wf_resolve_p7(int q, const WfClassLaunch& L);
 size_t wavefront_scratch_bytes(long long n, int n_slots);
 // Carve WfBuffers out of one block of at least wavefront_scratch_bytes(n, n_slots).
 WfBuffers wavefront_carve(void* base, long long n, int n_slots);
+
+// Launch shapes of the graph's per-round kernels (the autotuner's knobs).
+struct WfTuning {
+    long long step_blocks = 148 * 8;     // persistent k_wf_step_dev blocks of 128 (capped at one ray per thread)
+    long long scatter_blocks = 148 * 8;  // persistent k_wf_scatter_dev blocks of 256 (same)
+    int class_blocks = 0;               // k_wf_newton blocks of 256 per class launch; 0 = the plan's
+};
+
+// The whole intersection of n rays as one executable CUDA graph, in passes of
+// `chunk` rays.  Per pass: a set-up kernel, a while-loop node whose body is
+// one round (step, scan, scatter, one Newton kernel per degree class,
+// round_end, which sets the loop condition from the device-side count of
+// rays still traversing), then the resolve kernels.  No host
+// synchronisation; the graph is launched on any stream.  *passes gets the
+// number of passes.
+cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n,
+                                  long long chunk, const Opts& op, const Hits& out, const WfBuffers& wb,
+                                  unsigned long long* ctr, const WfTuning& tu, cudaGraphExec_t* exec,
+                                  long long* passes);
 
 // Runs the rounds; synchronises `stream` once per round to read the number of
 // rays still traversing into host_count (pinned host memory).

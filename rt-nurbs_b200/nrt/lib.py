@@ -77,6 +77,14 @@ class Counters(C.Structure):
         return d
 
 
+class Tuning(C.Structure):
+    _fields_ = [("step_blocks", C.c_int64), ("scatter_blocks", C.c_int64), ("class_blocks", C.c_int32),
+                ("graph", C.c_int32), ("chunk", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TrainOpts(C.Structure):
     _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("beta1", C.c_float),
                 ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint32)]
@@ -117,6 +125,10 @@ def lib():
         L.nrt_reference_opts.restype = None
         L.nrt_intersect.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts), C.POINTER(HitsC), vp]
         L.nrt_enable_counters.argtypes = [vp, C.c_int]
+        L.nrt_scene_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.nrt_scene_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.nrt_autotune.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts), C.POINTER(HitsC), C.c_int,
+                                   C.POINTER(Tuning), C.POINTER(C.c_float), vp]
         L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
         L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
         L.nrt_mlp_param_count.restype = C.c_size_t
@@ -272,6 +284,34 @@ class Scene:
         c = Counters()
         _check(lib().nrt_get_counters(self._h, C.byref(c), _stream_ptr(stream)))
         return c.as_dict()
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().nrt_scene_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Wavefront launch shapes (nrt_scene_set_tuning); unspecified fields are kept."""
+        t = Tuning(**{k: int(v) for k, v in kw.items()})
+        _check(lib().nrt_scene_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, rays, opts: IntersectOpts | None = None, out=None, reps=3, stream=None):
+        """nrt_autotune on these rays: keeps the fastest wavefront launch shapes on
+        the scene; returns (tuning dict, ms per call)."""
+        import torch
+
+        opts = opts or default_opts(schedule=SCHED_WAVEFRONT)
+        n = rays[0].numel()
+        if out is None:
+            out = {k: torch.empty(n, dtype=torch.int32 if k == "patch" else torch.float32, device=rays[0].device)
+                   for k in ("patch", "t", "u", "v")}
+        r = RaysC(*[C.c_void_p(a.data_ptr()) for a in rays])
+        h = HitsC(_ptr(out["patch"]), _ptr(out["t"]), _ptr(out["u"]), _ptr(out["v"]), _ptr(out.get("iters")),
+                  _ptr(out.get("tests")), _ptr(out.get("geom")))
+        t, ms = Tuning(), C.c_float()
+        _check(lib().nrt_autotune(self._h, C.byref(r), n, C.byref(opts), C.byref(h), int(reps), C.byref(t),
+                                  C.byref(ms), _stream_ptr(stream)))
+        return t.as_dict(), float(ms.value)
 
     def set_mlp(self, mlp: "Mlp"):
         _check(lib().nrt_scene_set_mlp(self._h, mlp.handle))

@@ -129,3 +129,34 @@ def test_clip_cull_changes_nothing(nrt_gpu):
         for k in ("patch", "t", "u", "v", "iters"):
             assert np.array_equal(base[k], b[k]), (k, level)
     assert culled[4] > culled[3] > culled[2] > culled[1] > 0, culled
+
+
+def test_tuning_changes_nothing_and_autotune(nrt_gpu):
+    """Launch shapes (graph or host-driven rounds, grid sizes, rays per pass)
+    change no result bit; the autotuner picks one of them."""
+    from nrt import scenes
+
+    sc = scenes.surfaces_grid_scene(16, seed=5, width=320, height=180, spp=2)
+    scene = nrt_gpu.Scene(sc.surfaces)
+    rays = nrt_gpu.camera_rays(sc.camera)
+    opts = nrt_gpu.default_opts(hull_cull=3, fp64_final=1, cond_fp64=1e4, schedule=nrt_gpu.SCHED_WAVEFRONT)
+    scene.enable_counters(True)
+    base = to_numpy(scene.intersect(rays, opts))
+    c0 = scene.counters()
+    assert c0["rounds"] > 1 and c0["kernel_launches"] > c0["rounds"]
+    for kw in [dict(graph=2), dict(graph=1, step_blocks=37, scatter_blocks=11, class_blocks=5),
+               dict(graph=1, chunk=10007), dict(graph=2, chunk=4096)]:
+        scene.set_tuning(**kw)
+        b = to_numpy(scene.intersect(rays, opts))
+        c = scene.counters()
+        for k in ("patch", "t", "u", "v", "iters", "tests"):
+            assert np.array_equal(base[k], b[k]), (k, kw)
+        assert c["newton_evals"] == c0["newton_evals"] and c["hits"] == c0["hits"], kw
+    scene.set_tuning(chunk=1 << 23)
+    scene.enable_counters(False)
+    t, ms = scene.autotune(rays, opts, reps=1)
+    assert ms > 0 and t["graph"] in (1, 2) and t["step_blocks"] > 0
+    assert scene.tuning() == t
+    b = to_numpy(scene.intersect(rays, opts))
+    for k in ("patch", "t", "u", "v", "iters"):
+        assert np.array_equal(base[k], b[k]), k
