@@ -42,13 +42,20 @@ def f_iter(p, q):
     return 12 * ((p + 1) * q * (q + 1) // 2 + p * (p + 1)) + 8 * (p + 2) + 80
 
 
-def algorithmic_flops(c):
-    fl = 12 * c["box_tests"] + 40 * c["rays"]
+def newton_flops(c):
+    """Algorithmic FP32 flops of the per-class Newton kernels: evaluations+steps
+    and the control-point hull tests (16 flops per point: two plane residuals)."""
+    fl = 0
     for (p, q), n in c["evals_by_degree"].items():
         fl += n * f_iter(p, q)
     for (p, q), n in c["hull_tests_by_degree"].items():
         fl += n * 16 * (p + 1) * (q + 1)
     return fl
+
+
+def algorithmic_flops(c):
+    """Whole step: box tests (12 flops), ray set-up (40 flops per ray) and the Newton kernels."""
+    return 12 * c["box_tests"] + 40 * c["rays"] + newton_flops(c)
 
 
 class ClockSampler:
@@ -282,6 +289,13 @@ def nrt_arm(args):
     cnt = scene.counters()
     scene.enable_counters(False)
     flops = algorithmic_flops(cnt)
+    # live device time of the dominant kernel family (the per-class Newton launches), CUDA events on the
+    # launching stream around each round's class launches; host-driven rounds for this measurement only
+    scene.enable_kernel_timing(True)
+    for _ in range(3):
+        step(best)
+    kt = scene.counters()
+    scene.enable_kernel_timing(False)
 
     with ClockSampler(local) as clk:
         ms_total = timed(best, args.steps, args.warmup)
@@ -342,13 +356,105 @@ def nrt_arm(args):
         e2e_ms = float(t.item())
     e2e_value = world * n * args.steps / (e2e_ms * 1e-3) / 1e6
 
+    # precision stress (7x7 rational patches, extreme weights, collapsed edges, 25% grazing rays):
+    # throughput and the share of FP64 work; its errors against the FP64 oracle are checked by
+    # tests/test_gpu_precision.py
+    prec_block = None
+    try:
+        (pcp, poff, pdeg), prays, _ = scenes.precision_workload(3840, 2160, seed=5)
+        pscene = nrt.Scene(patches=(pcp, poff, pdeg))
+        popts = nrt.default_opts(hull_cull=3, fp64_final=1, cond_fp64=1e4, schedule=nrt.SCHED_WAVEFRONT)
+        pn = prays[0].numel()
+        pout = {k: torch.empty(pn, dtype=v.dtype, device="cuda") for k, v in out.items()}
+        autotune.tune(pscene, prays, popts, out=pout)
+        pscene.enable_counters(True)
+        pscene.intersect(prays, popts, out=pout, stream=stream)
+        pc = pscene.counters()
+        pscene.enable_counters(False)
+        for _ in range(2):
+            pscene.intersect(prays, popts, out=pout, stream=stream)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(3):
+            pscene.intersect(prays, popts, out=pout, stream=stream)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        pms = s0.elapsed_time(s1) / 3
+        prec_block = {"workload": "32 rational 7x7 patches (w log-uniform 1e-2..1e2, 8 collapsed edges), "
+                                  "3840x2160 rays, 25% grazing (<= 2 deg)",
+                      "value": round(pn / (pms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(pms, 3),
+                      "hit_rate": round(pc["hits"] / pn, 4),
+                      "fp64_solve_frac": round(pc["fp64_solves"] / max(1, pc["newton_evals"]), 5),
+                      "fp64_final_steps_per_hit": round(pc["fp64_final_steps"] / max(1, pc["hits"]), 4),
+                      "newton_evals_per_ray": round(pc["newton_evals"] / pn, 3),
+                      "errors_vs_fp64_oracle": "tests/test_gpu_precision.py"}
+        pscene.close()
+        del prays, pout
+    except Exception as exc:  # reported, never silently replaced
+        prec_block = {"error": str(exc)[:200]}
+
+    # batched wavefront over bounce depths: 256 surfaces, 2048x2048x4 = 2^24 primary rays, then the
+    # depth-1 and depth-2 cosine-weighted bounces of the rays that hit (compacted, one nrt_intersect each)
+    bounce_block = None
+    if not args.no_bounce:
+        try:
+            wsc = scenes.wavefront_scene(3 + rank)
+            wscene = nrt.Scene(wsc.surfaces)
+            wrays = nrt.camera_rays(wsc.camera)
+            wn = wrays[0].numel()
+            wout = {"patch": torch.empty(wn, dtype=torch.int32, device="cuda"),
+                    "t": torch.empty(wn, dtype=torch.float32, device="cuda"),
+                    "u": torch.empty(wn, dtype=torch.float32, device="cuda"),
+                    "v": torch.empty(wn, dtype=torch.float32, device="cuda"),
+                    "geom": torch.empty((wn, 9), dtype=torch.float32, device="cuda")}
+            bufs = [([torch.empty(wn, dtype=torch.float32, device="cuda") for _ in range(6)],
+                     torch.empty(wn, dtype=torch.int32, device="cuda")) for _ in range(2)]
+            wtune, _ = autotune.tune(wscene, wrays, best, out=wout)
+
+            def batches():
+                cur, counts = wrays, []
+                for depth in range(3):
+                    wscene.intersect(cur, best, out={k: v[:cur[0].numel()] for k, v in wout.items()}, stream=stream)
+                    counts.append(cur[0].numel())
+                    if depth < 2:
+                        cur, _, _ = nrt.bounce_rays(cur, {k: v[:cur[0].numel()] for k, v in wout.items()},
+                                                    seed=17 + depth, offset=1e-4, out=bufs[depth], stream=stream)
+                return counts
+
+            batches()
+            torch.cuda.synchronize()
+            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b0.record(stream)
+            counts = batches()
+            b1.record(stream)
+            torch.cuda.synchronize()
+            bms = b0.elapsed_time(b1)
+            bounce_block = {"workload": f"256 NURBS surfaces deg 2-5 ({wscene.info()['n_patches']} Bezier patches), "
+                                        "2048x2048x4 = 2^24 primary rays + depth-1 and depth-2 diffuse bounces",
+                            "rays_per_depth": counts, "value": round(sum(counts) / (bms * 1e-3) / 1e6, 3),
+                            "unit": "Mrays/s", "ms": round(bms, 3), "tuning": wtune,
+                            "note": "time includes the bounce generation and its count read-back"}
+            wscene.close()
+            del wrays, wout, bufs
+        except Exception as exc:  # reported, never silently replaced
+            bounce_block = {"error": str(exc)[:200]}
+
     line = None
     if rank == 0:
-        achieved = flops / (ms_step * 1e-3) / 1e12
-        roof = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(sgemm, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / sgemm, 4), "traffic": ncu_traffic("wavefront_step"),
+        nl = max(1, kt["newton_kernel_launches"])
+        nfl = newton_flops(cnt)
+        k_ms = kt["newton_kernel_ms"] / nl
+        achieved = (nfl / nl) / (k_ms * 1e-3) / 1e12
+        step_achieved = flops / (ms_step * 1e-3) / 1e12
+        roof = {"bound": "fp32", "kernel": "k_wf_newton<P,Q> (one launch per degree class per round)",
+                "achieved": round(achieved, 3), "peak": round(sgemm, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / sgemm, 4), "traffic": ncu_traffic("k_wf_newton"),
                 "peak_source": "measured in this run: cuBLAS FP32 SGEMM 8192^3, TF32 off (burst)",
-                "flops_per_launch": int(flops),
+                "flops_per_launch": int(nfl / nl), "ms_per_launch": round(k_ms, 4), "launches_per_step": nl,
+                "kernel_share_of_step": round(kt["newton_kernel_ms"] / ms_step, 3),
+                "whole_step": {"achieved": round(step_achieved, 3), "frac": round(step_achieved / sgemm, 4),
+                               "flops_per_step": int(flops)},
                 "hbm": {"achieved_gbs": round(40.0 * n / (ms_step * 1e-3) / 1e9, 2),
                         "peak_gbs": peaks.get("hbm_gbs"), "algorithmic_bytes_per_ray": 40}}
         cpu = None
@@ -380,6 +486,8 @@ def nrt_arm(args):
                                "wavefront_rounds": cnt["rounds"], "kernels_per_step": cnt["kernel_launches"]},
                 "speedup_vs_plain_pixel": round(ms_plain / ms_step, 3),
                 "learned_init_wavefront": learned_block,
+                "precision_stress": prec_block,
+                "bounce_batches": bounce_block,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 24 * n,
                         "d2h_bytes_per_step": 16 * n},
@@ -397,6 +505,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nrt", choices=["nrt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-bounce", action="store_true", help="skip the 256-surface bounce-batch measurement")
     ap.add_argument("--profile", action="store_true", help="only launch the timed kernels (for ncu)")
     ap.add_argument("--profile-plain", action="store_true", help="with --profile: the plain per-pixel path")
     ap.add_argument("--spp", type=int, default=4,

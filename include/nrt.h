@@ -233,8 +233,16 @@ typedef struct {
     uint64_t hull_tests_by_degree[64]; /* hull tests per (p,q) */
     uint64_t kernel_launches;          /* kernels launched by the last nrt_intersect (host count) */
     uint64_t rounds;                   /* wavefront rounds of the last nrt_intersect */
+    double newton_kernel_ms;           /* with kernel timing on: device time of the per-class Newton
+                                          launches of the last nrt_intersect (CUDA events) */
+    uint64_t newton_kernel_launches;   /* with kernel timing on: how many such launches */
 } nrt_counters;
 int nrt_enable_counters(nrt_scene* scene, int enable);
+/* Kernel timing for roofline measurement: while enabled, the wavefront runs
+ * its rounds host-driven and brackets each round's per-class Newton launches
+ * with CUDA events on the caller's stream; nrt_get_counters reports their
+ * summed device time. */
+int nrt_enable_kernel_timing(nrt_scene* scene, int enable);
 int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream);
 
 /* ------------------------------------------------------------------------
@@ -250,6 +258,17 @@ typedef struct {
     uint32_t seed;
 } nrt_camera;
 int nrt_generate_camera_rays(const nrt_camera* cam, const nrt_rays_out* out, void* stream);
+
+/* Diffuse bounce rays from the hits of an nrt_intersect (no reference
+ * counterpart: the reference traces primary rays only).  For every ray with
+ * a hit, the shading normal normalize(dS/dv x dS/du) (the reference's normal,
+ * src/gpu/testShading.cu:46) turned against the incoming ray, a
+ * cosine-weighted direction about it from a PCG hash of (seed, ray index),
+ * and the origin S + offset * normal.  hits->geom is required.  The output is
+ * compacted in ray order: out[k], k < *n_out, with src_index[k] the input
+ * ray.  Synchronises `stream` (to return *n_out). */
+int nrt_generate_bounce_rays(const nrt_rays* rays, const nrt_hits* hits, int64_t n, uint32_t seed, float offset,
+                             const nrt_rays_out* out, int32_t* src_index, int64_t* n_out, void* stream);
 
 /* ------------------------------------------------------------------------
  * Learned initial guess (no reference counterpart: the reference starts every

@@ -271,14 +271,23 @@ struct nrt_scene {
     int32_t* host_count = nullptr;  // pinned word for the per-round active count
     long long last_launches = 0, last_rounds = 0;  // of the last nrt_intersect
     void* mlp_blob = nullptr;    // the scene's copy of the learned guess's network
-    // The wavefront as a CUDA graph: the last one built, the arguments it was
-    // built for (pointers, sizes, options, launch shapes) and its pass count.
-    cudaGraphExec_t wf_graph = nullptr;
-    std::vector<unsigned char> wf_graph_key;
-    long long wf_graph_passes = 0;
+    // The wavefront as CUDA graphs: the last few built (most recent last), each
+    // with the arguments it was built for (pointers, sizes, options, launch
+    // shapes) and its pass count.
+    struct WfGraph {
+        std::vector<unsigned char> key;
+        cudaGraphExec_t exec = nullptr;
+        long long passes = 0;
+    };
+    std::vector<WfGraph> wf_graphs;
+    long long wf_graph_passes = 0;  // passes of the graph the last call ran
     bool last_graph = false;     // the last nrt_intersect ran the graph (rounds counted on the device)
     dev::WfTuning tuning{};
     bool use_graph = true;       // false: host-driven rounds
+    bool timing_on = false;      // events around the per-class Newton launches (host-driven rounds)
+    cudaEvent_t tev[2] = {nullptr, nullptr};
+    double newton_ms = 0.0;
+    long long newton_launches = 0;
 };
 
 
@@ -596,7 +605,10 @@ int nrt_scene_destroy(nrt_scene* scene) {
     }
     if (scene->host_count) cudaFreeHost(scene->host_count);
     if (scene->mlp_blob) cudaFree(scene->mlp_blob);
-    if (scene->wf_graph) cudaGraphExecDestroy(scene->wf_graph);
+    for (auto& g : scene->wf_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (cudaEvent_t ev : scene->tev)
+        if (ev) cudaEventDestroy(ev);
     cudaSetDevice(prev);
     delete scene;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFree(scene)");
@@ -720,7 +732,17 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
         add(&scene->wf_rays, sizeof(scene->wf_rays));  // the scratch layout follows from it
         add(&d, sizeof(d));
         add(&scene->tuning, sizeof(scene->tuning));
-        if (!scene->use_graph) {
+        scene->newton_ms = 0.0;
+        scene->newton_launches = 0;
+        if (scene->timing_on && !scene->tev[0]) {
+            e = cudaEventCreate(&scene->tev[0]);
+            if (e == cudaSuccess) e = cudaEventCreate(&scene->tev[1]);
+            if (e != cudaSuccess) {
+                if (prev != scene->device) cudaSetDevice(prev);
+                return cuda_fail(e, "cudaEventCreate");
+            }
+        }
+        if (!scene->use_graph || scene->timing_on) {
             for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
                 const long long m = std::min(chunk, (long long)n - at);
                 dev::Rays rc{r.ox + at, r.oy + at, r.oz + at, r.dx + at, r.dy + at, r.dz + at};
@@ -729,22 +751,39 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
                 dev::Opts dc = d;
                 dc.seed_offset = d.seed_offset + (uint32_t)at;  // seeds follow the global ray index
                 e = dev::launch_wavefront(scene->view, scene->plan, rc, m, dc, hc, wb, scene->host_count,
-                                          scene->counters, st, &scene->last_launches, &scene->last_rounds);
+                                          scene->counters, st, &scene->last_launches, &scene->last_rounds,
+                                          scene->timing_on ? scene->tev : nullptr,
+                                          scene->timing_on ? &scene->newton_ms : nullptr, &scene->newton_launches);
             }
             if (prev != scene->device) cudaSetDevice(prev);
             if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
             return NRT_OK;
         }
-        if (!scene->wf_graph || key != scene->wf_graph_key) {
-            if (scene->wf_graph) cudaGraphExecDestroy(scene->wf_graph);
-            scene->wf_graph = nullptr;
-            scene->wf_graph_key.clear();
+        constexpr size_t kGraphsKept = 4;
+        auto& gs = scene->wf_graphs;
+        size_t at = 0;
+        while (at < gs.size() && gs[at].key != key) ++at;
+        if (at == gs.size()) {
+            nrt_scene::WfGraph g;
             e = dev::build_wavefront_graph(scene->view, scene->plan, r, (long long)n, chunk, d, h, wb,
-                                           scene->counters, scene->tuning, &scene->wf_graph,
-                                           &scene->wf_graph_passes);
-            if (e == cudaSuccess) scene->wf_graph_key = std::move(key);
+                                           scene->counters, scene->tuning, &g.exec, &g.passes);
+            if (e == cudaSuccess) {
+                g.key = std::move(key);
+                if (gs.size() == kGraphsKept) {  // drop the least recently used
+                    cudaGraphExecDestroy(gs.front().exec);
+                    gs.erase(gs.begin());
+                }
+                gs.push_back(std::move(g));
+                at = gs.size() - 1;
+            }
+        } else if (at + 1 != gs.size()) {  // most recent last
+            std::rotate(gs.begin() + at, gs.begin() + at + 1, gs.end());
+            at = gs.size() - 1;
         }
-        if (e == cudaSuccess) e = cudaGraphLaunch(scene->wf_graph, st);
+        if (e == cudaSuccess) {
+            e = cudaGraphLaunch(gs[at].exec, st);
+            scene->wf_graph_passes = gs[at].passes;
+        }
         scene->last_graph = true;
     }
     if (prev != scene->device) cudaSetDevice(prev);
@@ -861,6 +900,12 @@ int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_in
     return NRT_OK;
 }
 
+int nrt_enable_kernel_timing(nrt_scene* scene, int enable) {
+    if (!scene) return fail(NRT_ERR_INVALID, "null scene");
+    scene->timing_on = enable != 0;
+    return NRT_OK;
+}
+
 int nrt_enable_counters(nrt_scene* scene, int enable) {
     if (!scene) return fail(NRT_ERR_INVALID, "null scene");
     scene->counters_on = enable ? 1 : 0;
@@ -893,12 +938,40 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
         out->kernel_launches = (uint64_t)scene->last_launches;
         out->rounds = (uint64_t)scene->last_rounds;
     }
+    out->newton_kernel_ms = scene->newton_ms;
+    out->newton_kernel_launches = (uint64_t)scene->newton_launches;
     for (int k = 0; k < 64; ++k) {
         out->evals_by_degree[k] = h[dev::kEvalsByDegree + k];
         out->hull_tests_by_degree[k] = h[dev::kHullByDegree + k];
     }
     if (out->errors) return fail(NRT_ERR_DEVICE, "kernel reported %llu errors (traversal stack or degree)",
                                  (unsigned long long)out->errors);
+    return NRT_OK;
+}
+
+int nrt_generate_bounce_rays(const nrt_rays* rays, const nrt_hits* hits, int64_t n, uint32_t seed, float offset,
+                             const nrt_rays_out* out, int32_t* src_index, int64_t* n_out, void* stream) {
+    if (!rays || !hits || !out || !src_index || !n_out) return fail(NRT_ERR_INVALID, "null argument");
+    if (!hits->patch || !hits->geom) return fail(NRT_ERR_INVALID, "bounce rays need hits->patch and hits->geom");
+    if (!out->ox || !out->oy || !out->oz || !out->dx || !out->dy || !out->dz || !rays->dx || !rays->dy || !rays->dz)
+        return fail(NRT_ERR_INVALID, "null ray array");
+    if (n < 0 || n > (1LL << 31) - 256) return fail(NRT_ERR_INVALID, "ray count %lld outside 0..2^31-256", (long long)n);
+    *n_out = 0;
+    if (n == 0) return NRT_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long nb = (n + 255) / 256;
+    int32_t* scratch = nullptr;
+    NRT_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&scratch), (nb + 1) * sizeof(int32_t), st), "cudaMallocAsync");
+    const nrt::dev::Rays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz};
+    cudaError_t e = nrt::dev::launch_bounce_rays(r, hits->patch, hits->geom, n, seed, offset, out->ox, out->oy, out->oz,
+                                                 out->dx, out->dy, out->dz, src_index, scratch, st);
+    int32_t total = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, scratch + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    const cudaError_t ef = cudaFreeAsync(scratch, st);
+    if (e == cudaSuccess) e = ef;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "bounce rays");
+    *n_out = total;
     return NRT_OK;
 }
 

@@ -27,6 +27,10 @@ struct CameraParams {
 };
 cudaError_t launch_camera_rays(const CameraParams& cp, float* ox, float* oy, float* oz, float* dx, float* dy,
                                float* dz, cudaStream_t stream);
+// Compacted diffuse bounce rays of the hits (scratch: (n + 255) / 256 + 1 ints).
+cudaError_t launch_bounce_rays(const Rays& in, const int32_t* patch, const float* geom, long long n, uint32_t seed,
+                               float offset, float* ox, float* oy, float* oz, float* dx, float* dy, float* dz,
+                               int32_t* src, int32_t* scratch, cudaStream_t stream);
 
 }  // namespace dev
 }  // namespace nrt

@@ -38,6 +38,7 @@ struct RayFrame {
 struct PatchRay {
     float e1, e2, tc;
     double e1d, e2d, tcd;
+    double ocx, ocy, ocz;  // ray origin minus patch centre, in double (the FP64 final step)
 };
 
 struct NewtonOpts {
@@ -86,6 +87,9 @@ __device__ __forceinline__ PatchRay patch_ray(const RayFrame& r, double cx, doub
     pr.e1d = -((double)r.n1x * ox + (double)r.n1y * oy + (double)r.n1z * oz);
     pr.e2d = -((double)r.n2x * ox + (double)r.n2y * oy + (double)r.n2z * oz);
     pr.tcd = -((double)r.dx * ox + (double)r.dy * oy + (double)r.dz * oz);
+    pr.ocx = ox;
+    pr.ocy = oy;
+    pr.ocz = oz;
     pr.e1 = (float)pr.e1d;
     pr.e2 = (float)pr.e2d;
     pr.tc = (float)pr.tcd;
@@ -483,45 +487,99 @@ __device__ __forceinline__ bool obb_misses(const float4* __restrict__ obb, const
     return tf < tn;
 }
 
-// One FP64 Newton step from a converged (u, v): evaluate in double, solve the
-// 2x2 system exactly in double, clamp, and move S to first order.
+// FP64 refinement of a converged (u, v): the ray's planes are rebuilt in
+// double from the (float) ray (the FP32 planes are off the ray by an
+// ulp-sized angle, which a grazing ray turns into a t shift), then up to six
+// Newton steps in double (near-singular Jacobians of grazing rays converge
+// slowly), each re-evaluating the patch, for as long as the residual
+// decreases; the point with the smallest residual is kept, so the step never
+// makes a converged FP32 hit worse.  A step below 1e-7 in (u, v) ends the
+// refinement with a first-order move of S (no further evaluation): that is
+// the common case, one FP64 evaluation per hit.  S, dS/du, dS/dv and t are
+// those of the final (u, v), in double.
 template <int P, int Q>
 __device__ __forceinline__ void final_step_fp64(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
                                                 NewtonOut& o) {
-    double H[4], Hu[4], Hv[4];
-    eval_patch_fp64<P, Q>(blk, (double)o.u, (double)o.v, H, Hu, Hv);
-    const double iw = 1.0 / H[3];
-    const double S[3] = {H[0] * iw, H[1] * iw, H[2] * iw};
-    double Su[3], Sv[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        Su[a] = (Hu[a] - S[a] * Hu[3]) * iw;
-        Sv[a] = (Hv[a] - S[a] * Hv[3]) * iw;
+    const double dx = r.dx, dy = r.dy, dz = r.dz;
+    const double ax = fabs(dx), ay = fabs(dy), az = fabs(dz);
+    double n1[3], n2[3];
+    if (ax > ay && ax > az) {
+        const double l = sqrt(dx * dx + dy * dy);
+        n1[0] = dy / l; n1[1] = -dx / l; n1[2] = 0.0;
+    } else {
+        const double l = sqrt(dy * dy + dz * dz);
+        n1[0] = 0.0; n1[1] = dz / l; n1[2] = -dy / l;
     }
-    const double n1[3] = {r.n1x, r.n1y, r.n1z}, n2[3] = {r.n2x, r.n2y, r.n2z};
-    const double r1 = n1[0] * S[0] + n1[1] * S[1] + n1[2] * S[2] + pr.e1d;
-    const double r2 = n2[0] * S[0] + n2[1] * S[1] + n2[2] * S[2] + pr.e2d;
-    const double j11 = n1[0] * Su[0] + n1[1] * Su[1] + n1[2] * Su[2];
-    const double j21 = n2[0] * Su[0] + n2[1] * Su[1] + n2[2] * Su[2];
-    const double j12 = n1[0] * Sv[0] + n1[1] * Sv[1] + n1[2] * Sv[2];
-    const double j22 = n2[0] * Sv[0] + n2[1] * Sv[1] + n2[2] * Sv[2];
-    const double det = j11 * j22 - j12 * j21;
-    double du = 0.0, dv = 0.0;
-    if (det != 0.0) {
-        du = (j22 * r1 - j12 * r2) / det;
-        dv = (j11 * r2 - j21 * r1) / det;
-    }
-    const double un = fmin(fmax((double)o.u - du, 0.0), 1.0), vn = fmin(fmax((double)o.v - dv, 0.0), 1.0);
-    const double su = un - (double)o.u, sv = vn - (double)o.v;
-    double Sn[3];
+    const double il = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+    const double ux = dx * il, uy = dy * il, uz = dz * il;
+    n2[0] = n1[1] * uz - n1[2] * uy;
+    n2[1] = n1[2] * ux - n1[0] * uz;
+    n2[2] = n1[0] * uy - n1[1] * ux;
+    const double oc[3] = {pr.ocx, pr.ocy, pr.ocz};
+    const double e1 = -(n1[0] * oc[0] + n1[1] * oc[1] + n1[2] * oc[2]);
+    const double e2 = -(n2[0] * oc[0] + n2[1] * oc[1] + n2[2] * oc[2]);
+    double u = o.u, v = o.v;
+    double H[4], Hu[4], Hv[4], S[3], Su[3], Sv[3];
+    auto eval = [&]() {
+        eval_patch_fp64<P, Q>(blk, u, v, H, Hu, Hv);
+        const double iw = 1.0 / H[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) Sn[a] = S[a] + Su[a] * su + Sv[a] * sv;
-    const double d[3] = {r.dx, r.dy, r.dz};
-    const double t = Sn[0] * d[0] + Sn[1] * d[1] + Sn[2] * d[2] + pr.tcd;
-    o.u = (float)un;
-    o.v = (float)vn;
+        for (int a = 0; a < 3; ++a) {
+            S[a] = H[a] * iw;
+            Su[a] = (Hu[a] - S[a] * Hu[3]) * iw;
+            Sv[a] = (Hv[a] - S[a] * Hv[3]) * iw;
+        }
+    };
+    auto residual = [&](double& r1, double& r2) {
+        r1 = n1[0] * S[0] + n1[1] * S[1] + n1[2] * S[2] + e1;
+        r2 = n2[0] * S[0] + n2[1] * S[1] + n2[2] * S[2] + e2;
+        return fabs(r1) + fabs(r2);
+    };
+    eval();
+    double r1, r2;
+    double best = residual(r1, r2);
+    double bu = u, bv = v, bS[3] = {S[0], S[1], S[2]}, bSu[3] = {Su[0], Su[1], Su[2]}, bSv[3] = {Sv[0], Sv[1], Sv[2]};
+#pragma unroll 1
+    for (int it = 0; it < 6 && best > 0.0; ++it) {
+        const double j11 = n1[0] * Su[0] + n1[1] * Su[1] + n1[2] * Su[2];
+        const double j21 = n2[0] * Su[0] + n2[1] * Su[1] + n2[2] * Su[2];
+        const double j12 = n1[0] * Sv[0] + n1[1] * Sv[1] + n1[2] * Sv[2];
+        const double j22 = n2[0] * Sv[0] + n2[1] * Sv[1] + n2[2] * Sv[2];
+        const double det = j11 * j22 - j12 * j21;
+        if (det == 0.0) break;
+        const double du = (j22 * r1 - j12 * r2) / det, dv = (j11 * r2 - j21 * r1) / det;
+        const double un = fmin(fmax(u - du, 0.0), 1.0), vn = fmin(fmax(v - dv, 0.0), 1.0);
+        if (fabs(un - u) + fabs(vn - v) < 1e-7) {
+            // a small step: its second-order remainder is below float resolution, so the point
+            // moves to first order without another evaluation
+            const double su = un - u, sv = vn - v;
+            u = un;
+            v = vn;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) S[a] += Su[a] * su + Sv[a] * sv;
+            bu = u; bv = v;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) { bS[a] = S[a]; bSu[a] = Su[a]; bSv[a] = Sv[a]; }
+            break;
+        }
+        u = un;
+        v = vn;
+        eval();
+        const double res = residual(r1, r2);
+        if (!(res < best)) break;  // no progress (or a jump away): keep the best point so far
+        best = res;
+        bu = u; bv = v;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { bS[a] = S[a]; bSu[a] = Su[a]; bSv[a] = Sv[a]; }
+    }
+    u = bu; v = bv;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { S[a] = bS[a]; Su[a] = bSu[a]; Sv[a] = bSv[a]; }
+    const double t = (S[0] - oc[0]) * dx + (S[1] - oc[1]) * dy + (S[2] - oc[2]) * dz;
+    o.u = (float)u;
+    o.v = (float)v;
     o.t = (float)t;
-    o.sx = (float)Sn[0]; o.sy = (float)Sn[1]; o.sz = (float)Sn[2];
+    o.sx = (float)S[0]; o.sy = (float)S[1]; o.sz = (float)S[2];
     o.ux = (float)Su[0]; o.uy = (float)Su[1]; o.uz = (float)Su[2];
     o.vx = (float)Sv[0]; o.vy = (float)Sv[1]; o.vz = (float)Sv[2];
     o.fp64_final = 1;

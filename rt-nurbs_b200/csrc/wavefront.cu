@@ -397,7 +397,8 @@ static void wf_resolve_class(int p, int q, const WfClassLaunch& L) {
 
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
-                             cudaStream_t stream, long long* launches, long long* rounds) {
+                             cudaStream_t stream, long long* launches, long long* rounds, cudaEvent_t* ev,
+                             double* newton_ms, long long* newton_launches) {
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     int n_active = (int)n, cur = 0;
@@ -418,6 +419,8 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
                                                                              plan.rank_of);
         *launches += 3 + plan.n_classes;
         *rounds += 1;
+        const bool timed = ev && newton_ms;
+        if (timed) cudaEventRecord(ev[0], stream);
         for (int c = 0; c < plan.n_classes; ++c) {
             L.cls = c;
             L.rank_lo = plan.class_rank[c];
@@ -425,9 +428,17 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
             L.grid = plan.class_grid[c];
             wf_newton_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
         }
+        if (timed) cudaEventRecord(ev[1], stream);
         e = cudaMemcpyAsync(host_count, wb.counts + (1 - cur), sizeof(int), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return e;
+        if (timed) {
+            float ms = 0.f;
+            e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            if (e != cudaSuccess) return e;
+            *newton_ms += ms;
+            if (newton_launches) *newton_launches += plan.n_classes;
+        }
         n_active = *host_count;
         cur = 1 - cur;
     }

@@ -114,9 +114,12 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
 
 // Runs the rounds; synchronises `stream` once per round to read the number of
 // rays still traversing into host_count (pinned host memory).
+// With ev[2] (two events) and newton_ms, each round's per-class Newton
+// launches are bracketed by the events and their time added to *newton_ms.
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
-                             cudaStream_t stream, long long* launches, long long* rounds);
+                             cudaStream_t stream, long long* launches, long long* rounds,
+                             cudaEvent_t* ev = nullptr, double* newton_ms = nullptr, long long* newton_launches = nullptr);
 
 // Per-pixel kernel over a device list of ray indices (count read on the device).
 cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const int32_t* list,

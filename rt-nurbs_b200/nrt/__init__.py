@@ -14,6 +14,7 @@ from .lib import (  # noqa: F401
     Mlp,
     NrtError,
     Scene,
+    bounce_rays,
     build_bvh_binary,
     camera_rays,
     decompose,

@@ -66,7 +66,9 @@ _COUNTER_NAMES = ("rays", "box_tests", "patch_candidates", "patch_culled", "newt
 class Counters(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in _COUNTER_NAMES] + [("evals_by_degree", C.c_uint64 * 64),
                                                             ("hull_tests_by_degree", C.c_uint64 * 64),
-                                                            ("kernel_launches", C.c_uint64), ("rounds", C.c_uint64)]
+                                                            ("kernel_launches", C.c_uint64), ("rounds", C.c_uint64),
+                                                            ("newton_kernel_ms", C.c_double),
+                                                            ("newton_kernel_launches", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: int(getattr(self, k)) for k in _COUNTER_NAMES}
@@ -74,6 +76,8 @@ class Counters(C.Structure):
         d["hull_tests_by_degree"] = {(k // 8, k % 8): int(v) for k, v in enumerate(self.hull_tests_by_degree) if v}
         d["kernel_launches"] = int(self.kernel_launches)
         d["rounds"] = int(self.rounds)
+        d["newton_kernel_ms"] = float(self.newton_kernel_ms)
+        d["newton_kernel_launches"] = int(self.newton_kernel_launches)
         return d
 
 
@@ -125,12 +129,15 @@ def lib():
         L.nrt_reference_opts.restype = None
         L.nrt_intersect.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts), C.POINTER(HitsC), vp]
         L.nrt_enable_counters.argtypes = [vp, C.c_int]
+        L.nrt_enable_kernel_timing.argtypes = [vp, C.c_int]
         L.nrt_scene_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.nrt_scene_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.nrt_autotune.argtypes = [vp, C.POINTER(RaysC), C.c_int64, C.POINTER(IntersectOpts), C.POINTER(HitsC), C.c_int,
                                    C.POINTER(Tuning), C.POINTER(C.c_float), vp]
         L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
         L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
+        L.nrt_generate_bounce_rays.argtypes = [C.POINTER(RaysC), C.POINTER(HitsC), C.c_int64, C.c_uint32, C.c_float,
+                                               C.POINTER(RaysC), vp, C.POINTER(C.c_int64), vp]
         L.nrt_mlp_param_count.restype = C.c_size_t
         L.nrt_mlp_create.argtypes = [C.c_int, C.c_uint32, C.POINTER(vp)]
         L.nrt_mlp_destroy.argtypes = [vp]
@@ -285,6 +292,9 @@ class Scene:
         _check(lib().nrt_get_counters(self._h, C.byref(c), _stream_ptr(stream)))
         return c.as_dict()
 
+    def enable_kernel_timing(self, on=True):
+        _check(lib().nrt_enable_kernel_timing(self._h, int(on)))
+
     def tuning(self) -> dict:
         t = Tuning()
         _check(lib().nrt_scene_get_tuning(self._h, C.byref(t)))
@@ -356,6 +366,28 @@ class Scene:
                   _ptr(out.get("tests")), _ptr(out.get("geom")))
         _check(lib().nrt_intersect(self._h, C.byref(r), n, C.byref(opts), C.byref(h), _stream_ptr(stream)))
         return out
+
+
+def bounce_rays(rays, hits, seed=0, offset=1e-4, out=None, stream=None):
+    """nrt_generate_bounce_rays: (6 ray tensors of length m, source-index tensor, m) for the
+    rays that hit; hits must carry "geom" (intersect(..., geom=True))."""
+    import torch
+
+    n = rays[0].numel()
+    dev = rays[0].device
+    if out is None:
+        out = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(6)]
+        src = torch.empty(n, dtype=torch.int32, device=dev)
+    else:
+        out, src = out
+    r = RaysC(*[C.c_void_p(a.data_ptr()) for a in rays])
+    h = HitsC(_ptr(hits["patch"]), _ptr(hits["t"]), _ptr(hits["u"]), _ptr(hits["v"]), None, None, _ptr(hits["geom"]))
+    o = RaysC(*[C.c_void_p(a.data_ptr()) for a in out])
+    m = C.c_int64()
+    _check(lib().nrt_generate_bounce_rays(C.byref(r), C.byref(h), n, int(seed) & 0xFFFFFFFF, float(offset), C.byref(o),
+                                          _ptr(src), C.byref(m), _stream_ptr(stream)))
+    k = int(m.value)
+    return [a[:k] for a in out], src[:k], k
 
 
 class Camera(CameraC):

@@ -219,3 +219,117 @@ def wavefront_scene(seed: int = 3, width: int = 2048, height: int = 2048, spp: i
     """256 surfaces from the same generator (about 40k-100k Bezier patches);
     2048x2048 with 4 jittered samples (2^24 primary rays per batch)."""
     return surfaces_grid_scene(256, seed, width, height, spp, name="wave256")
+
+
+# --------------------------------------------------------------------------
+# Precision stress: degree 7x7 rational patches, extreme weights, collapsed
+# edges, grazing rays.
+def _bernstein(n: int, t: np.ndarray):
+    """Bernstein values and derivatives of degree n at t (float64), shape (len(t), n+1)."""
+    from math import comb
+
+    k = np.arange(n + 1)
+    c = np.array([comb(n, i) for i in k], np.float64)
+    t = t[:, None]
+    B = c * t ** k * (1.0 - t) ** (n - k)
+    km = np.arange(n)
+    cm = np.array([comb(n - 1, i) for i in km], np.float64)
+    Bm = cm * t ** km * (1.0 - t) ** (n - 1 - km)
+    dB = np.zeros_like(B)
+    dB[:, :-1] -= n * Bm
+    dB[:, 1:] += n * Bm
+    return B, dB
+
+
+def patch_points(cp: np.ndarray, p: int, q: int, u: np.ndarray, v: np.ndarray):
+    """S, dS/du, dS/dv (float64) of rational Bezier patches cp[k] ((p+1)(q+1) x 4,
+    weighted-homogeneous, index i*(q+1)+j) at (u[k], v[k])."""
+    P = cp.reshape(-1, p + 1, q + 1, 4).astype(np.float64)
+    Bu, dBu = _bernstein(p, u)
+    Bv, dBv = _bernstein(q, v)
+    H = np.einsum("ki,kj,kijc->kc", Bu, Bv, P)
+    Hu = np.einsum("ki,kj,kijc->kc", dBu, Bv, P)
+    Hv = np.einsum("ki,kj,kijc->kc", Bu, dBv, P)
+    w = H[:, 3:4]
+    S = H[:, :3] / w
+    return S, (Hu[:, :3] - S * Hu[:, 3:4]) / w, (Hv[:, :3] - S * Hv[:, 3:4]) / w
+
+
+def precision_patches(seed: int = 5, n_patches: int = 32, collapsed: int = 8):
+    """n_patches rational Bezier patches of degree 7x7 on an 8-wide wall of unit
+    squares (spacing 1.1) facing -y, gentle random relief, weights log-uniform
+    in [1e-2, 1e2]; the first `collapsed` patches have their u = 0 edge
+    collapsed to one point (a degenerate, triangle-like net).  Returns
+    (cp (n*64, 4) float32 weighted-homogeneous, offsets, degrees)."""
+    rng = np.random.default_rng(seed)
+    p = q = 7
+    cps, off, deg = [], [], []
+    cols = 8
+    for k in range(n_patches):
+        ix, iz = k % cols, k // cols
+        g = np.linspace(0.0, 1.0, p + 1)
+        X, Z = np.meshgrid(g, g, indexing="ij")
+        Y = 0.15 * rng.normal(size=X.shape)
+        xyz = np.stack([X + 1.1 * ix - 0.55 * cols, Y, Z + 1.1 * iz - 0.55 * (n_patches // cols)], -1)
+        if k < collapsed:
+            xyz[0, :, :] = xyz[0, (q + 1) // 2, :]  # the whole u = 0 row at one point
+        w = 10.0 ** rng.uniform(-2.0, 2.0, (p + 1) * (q + 1))
+        cps.append(_homogeneous(xyz.reshape(-1, 3), w))
+        off.append(k * (p + 1) * (q + 1))
+        deg.append((p, q))
+    return np.concatenate(cps), np.array(off, np.int32), np.array(deg, np.int32)
+
+
+def precision_camera(width: int = 3840, height: int = 2160, seed: int = 5) -> Camera:
+    """A pinhole camera in front of the precision wall (pixel-centre rays)."""
+    return Camera((0.3, -7.0, 0.4), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 40.0, width, height, 1, seed)
+
+
+def grazing_rays(cp: np.ndarray, off: np.ndarray, deg: np.ndarray, m: int, seed: int = 5, max_deg: float = 2.0):
+    """m rays within max_deg degrees of a patch's tangent plane: a surface point
+    S is drawn (random patch, (u, v) in [0.05, 0.95]^2, FP64), a direction d
+    at U(0, max_deg) degrees from a random tangent direction towards the
+    patch's front (-y) side, and the origin backed off along it by U(1, 3):
+    O = S - L d.  Returns float32 arrays (ox, oy, oz, dx, dy, dz)."""
+    rng = np.random.default_rng(seed + 1000)
+    k = rng.integers(0, len(off), m)
+    p, q = int(deg[0, 0]), int(deg[0, 1])
+    n_pts = (p + 1) * (q + 1)
+    blocks = np.stack([cp[off[i]:off[i] + n_pts] for i in range(len(off))])[k]
+    u = rng.uniform(0.05, 0.95, m)
+    v = rng.uniform(0.05, 0.95, m)
+    S, Su, Sv = patch_points(blocks.reshape(m, -1), p, q, u, v)
+    nrm = np.cross(Su, Sv)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True) + 1e-300
+    nrm *= np.where(nrm[:, 1:2] > 0, -1.0, 1.0)  # towards the front (-y)
+    t1 = Su / (np.linalg.norm(Su, axis=1, keepdims=True) + 1e-300)
+    t2 = np.cross(nrm, t1)
+    phi = rng.uniform(0.0, 2.0 * np.pi, m)[:, None]
+    tang = np.cos(phi) * t1 + np.sin(phi) * t2
+    a = np.radians(rng.uniform(0.0, max_deg, m))[:, None]
+    d = np.cos(a) * tang - np.sin(a) * nrm  # enters the surface from the front
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    L = rng.uniform(1.0, 3.0, m)[:, None]
+    o = S - L * d
+    return tuple(np.ascontiguousarray(x, np.float32) for x in (o[:, 0], o[:, 1], o[:, 2], d[:, 0], d[:, 1], d[:, 2]))
+
+
+def precision_workload(width: int = 3840, height: int = 2160, seed: int = 5, grazing: float = 0.25):
+    """The precision-stress workload: the patches of precision_patches, camera
+    rays of precision_camera with every round(1/grazing)-th ray replaced by a
+    grazing ray.  Returns (patches (cp, off, deg), rays as 6 float32 CUDA
+    tensors, indices of the grazing rays)."""
+    import torch
+
+    from . import lib_module as L
+
+    cp, off, deg = precision_patches(seed)
+    rays = L.camera_rays(precision_camera(width, height, seed))
+    n = rays[0].numel()
+    step = max(1, int(round(1.0 / grazing)))
+    idx = np.arange(0, n, step)
+    g = grazing_rays(cp, off, deg, idx.size, seed)
+    ti = torch.from_numpy(idx).to(rays[0].device)
+    for a, b in zip(rays, g):
+        a[ti] = torch.from_numpy(b).to(a.device)
+    return (cp, off, deg), rays, idx

@@ -1,0 +1,122 @@
+"""Precision stress on the GPU (through the C ABI): 32 rational 7x7 patches
+with weights log-uniform in [1e-2, 1e2], 8 of them with a collapsed edge,
+960x540 camera rays of which 25% graze a patch (within 2 degrees of its
+tangent plane).  FP32 Newton with the FP64 escalation (2x2 solve in FP64 when
+cond(J) > 1e4) and the FP64 final step.
+
+Two references:
+  * the FP64 oracle (the same method in double, TEST INFRASTRUCTURE) judges
+    hit/miss.  On these nets Newton's basins are chaotic (degree 7, a 1e4
+    weight ratio, steep relief): FP32 and FP64 iterations from the same start
+    part ways on a fraction of a percent of rays, with or without the FP64
+    steps, so agreement is asserted at >= 99% and reported;
+  * the exact root next to each GPU hit (FP64 Newton from the GPU's (u, v),
+    converged to 1e-13 in double, numpy) gives the t and (u, v) error of the
+    returned hits.  With the FP64 final step: relative t error <= 5e-6 at the
+    99.9th and <= 2e-5 at the 99.99th percentile, above 1e-4 on at most 1e-4
+    of the hits and never above 2e-3, (u, v) error <= 1e-4 at the 99.99th
+    percentile; the 99.99th-percentile t error at most a tenth of FP32 alone.
+The escalation must run (FP64 solves > 0) and every hit takes the final step.
+"""
+import numpy as np
+import pytest
+
+from parity import compare, to_numpy
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nrt_gpu():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import nrt
+
+    nrt.lib()
+    return nrt
+
+
+def _planes(o, d):
+    """The reference's two ray planes (src/math/math_utils.h:33-54), in double."""
+    a = np.abs(d)
+    xdom = (a[:, 0] > a[:, 1]) & (a[:, 0] > a[:, 2])
+    n1 = np.where(xdom[:, None], np.stack([d[:, 1], -d[:, 0], 0 * d[:, 0]], 1),
+                  np.stack([0 * d[:, 0], d[:, 2], -d[:, 1]], 1))
+    n1 /= np.linalg.norm(n1, axis=1, keepdims=True)
+    n2 = np.cross(n1, d / np.linalg.norm(d, axis=1, keepdims=True))
+    return n1, -np.sum(n1 * o, 1), n2, -np.sum(n2 * o, 1)
+
+
+def exact_roots(blocks, p, q, o, d, u, v, iters=30):
+    """FP64 Newton on the two ray planes from (u, v), clamped to [0,1]^2 as the
+    method does, to |r| < 1e-13; returns (u, v, t, converged)."""
+    from nrt.scenes import patch_points
+
+    n1, d1, n2, d2 = _planes(o, d)
+    u, v = u.astype(np.float64).copy(), v.astype(np.float64).copy()
+    ok = np.zeros(len(u), bool)
+    for _ in range(iters):
+        S, Su, Sv = patch_points(blocks, p, q, u, v)
+        r1, r2 = np.sum(n1 * S, 1) + d1, np.sum(n2 * S, 1) + d2
+        ok = np.abs(r1) + np.abs(r2) < 1e-13
+        a, b, c, e = np.sum(n1 * Su, 1), np.sum(n1 * Sv, 1), np.sum(n2 * Su, 1), np.sum(n2 * Sv, 1)
+        det = a * e - b * c
+        det = np.where(det == 0, 1.0, det)
+        u = np.where(ok, u, np.clip(u - (e * r1 - b * r2) / det, 0, 1))
+        v = np.where(ok, v, np.clip(v - (-c * r1 + a * r2) / det, 0, 1))
+    S, _, _ = patch_points(blocks, p, q, u, v)
+    return u, v, np.sum((S - o) * d, 1), ok
+
+
+def hit_errors(out, cp, off, rays_np):
+    hit = np.nonzero(out["patch"] >= 0)[0]
+    k = out["patch"][hit]
+    blocks = np.stack([cp[off[j]:off[j] + 64] for j in range(len(off))])[k].reshape(len(hit), -1)
+    o = np.stack(rays_np[:3], 1)[hit].astype(np.float64)
+    d = np.stack(rays_np[3:], 1)[hit].astype(np.float64)
+    u, v, t, ok = exact_roots(blocks, 7, 7, o, d, out["u"][hit], out["v"][hit])
+    rel_t = np.abs(out["t"][hit].astype(np.float64) - t) / np.abs(t)
+    duv = np.maximum(np.abs(out["u"][hit] - u), np.abs(out["v"][hit] - v))
+    return rel_t[ok], duv[ok], float(ok.mean())
+
+
+def test_precision_stress(nrt_gpu, oracle_mod):
+    from nrt import scenes
+
+    (cp, off, deg), rays, graze = scenes.precision_workload(960, 540, seed=5)
+    scene = nrt_gpu.Scene(patches=(cp, off, deg))
+    opts = nrt_gpu.default_opts(hull_cull=3, fp64_final=1, cond_fp64=1e4, schedule=nrt_gpu.SCHED_WAVEFRONT)
+    scene.enable_counters(True)
+    out = to_numpy(scene.intersect(rays, opts))
+    c = scene.counters()
+    fp32 = to_numpy(scene.intersect(rays, opts.replace(fp64_final=0, cond_fp64=0.0)))
+    rays_np = [a.cpu().numpy() for a in rays]
+    # hit/miss against the same method in FP64
+    P = oracle_mod.Patches(cp, off, deg, np.zeros((len(off), 4), np.float32), np.zeros(len(off), np.int32),
+                           cp.astype(np.float64))
+    bvh = oracle_mod.build_bvh(oracle_mod.patch_boxes(P))
+    ref = oracle_mod.intersect(P, bvh, oracle_mod.Rays(*rays_np), 0, 8, 1e-6, f64=True)
+    st = compare(out, ref.patch, ref.t, ref.u, ref.v)
+    sel = np.zeros(out["patch"].size, bool)
+    sel[graze] = True
+    stg = compare({k: v[sel] for k, v in out.items()}, ref.patch[sel], ref.t[sel], ref.u[sel], ref.v[sel])
+    # accuracy of the returned hits against the exact roots next to them
+    rel, duv, conv = hit_errors(out, cp, off, rays_np)
+    rel32, duv32, _ = hit_errors(fp32, cp, off, rays_np)
+    fp64_frac = c["fp64_solves"] / max(1, c["newton_evals"])
+    print("precision stress: agreement", round(st["agree"], 6), "grazing", round(stg["agree"], 6),
+          "hit rate", round(st["hit_rate"], 4), "| t rel err: max", rel.max(), "p99.99", np.quantile(rel, 0.9999),
+          "p99.9", np.quantile(rel, 0.999), "gt1e-4", (rel > 1e-4).sum(), "of", rel.size,
+          "| uv err: max", duv.max(), "p99.99", np.quantile(duv, 0.9999), "| FP32 only: t max", rel32.max(),
+          "p99.99", np.quantile(rel32, 0.9999), "uv p99.99", np.quantile(duv32, 0.9999),
+          "| FP64 solve fraction", round(fp64_frac, 5), "| exact root found for", round(conv, 5))
+    assert st["hit_rate"] > 0.2 and stg["hit_rate"] > 0.5, (st, stg)
+    assert st["agree"] >= 0.99 and stg["agree"] >= 0.99, (st, stg)
+    assert conv > 0.999
+    assert np.quantile(rel, 0.999) <= 5e-6 and np.quantile(rel, 0.9999) <= 2e-5, np.quantile(rel, [0.999, 0.9999])
+    assert (rel > 1e-4).mean() <= 1e-4 and rel.max() <= 2e-3, ((rel > 1e-4).sum(), rel.max())
+    assert np.quantile(duv, 0.9999) <= 1e-4, np.quantile(duv, 0.9999)
+    assert np.quantile(rel, 0.9999) < 0.1 * np.quantile(rel32, 0.9999)
+    assert c["fp64_solves"] > 0 and c["fp64_final_steps"] == c["hits"], c
