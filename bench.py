@@ -210,26 +210,19 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------
 def nrt_arm(args):
     import torch
-    import torch.distributed as dist
 
     import nrt
     from nrt import scenes
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from nrt import dist as ndist
+
+    rank, world, local = ndist.env_ranks()
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    ndist.init("nccl", timeout_s=120)
+    barrier = ndist.barrier
 
     sc = scenes.mixed_degree_scene(1, spp=args.spp)
-    sc.camera.seed = 1 + rank  # each rank its own samples
+    sc.camera.seed = ndist.rank_seed(1, rank)  # each rank its own samples
     t0 = time.perf_counter()
     scene = nrt.Scene(sc.surfaces)
     build_s = time.perf_counter() - t0
@@ -259,12 +252,7 @@ def nrt_arm(args):
         e.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = s.elapsed_time(e)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return ndist.max_over_ranks(s.elapsed_time(e), device="cuda")
 
     if args.profile:
         # only the path's kernels, for ncu: warmup + steps launches of the timed configuration, with
@@ -300,7 +288,7 @@ def nrt_arm(args):
     with ClockSampler(local) as clk:
         ms_total = timed(best, args.steps, args.warmup)
     ms_step = ms_total / args.steps
-    value = world * n * args.steps / (ms_total * 1e-3) / 1e6
+    value = ndist.weak_scaling_rate(n * args.steps, world, ms_total * 1e-3) / 1e6
 
     ms_plain = timed(plain, max(1, args.steps // 2), 1) / max(1, args.steps // 2)
 
@@ -349,12 +337,8 @@ def nrt_arm(args):
     e.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = s.elapsed_time(e)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n * args.steps / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = ndist.max_over_ranks(s.elapsed_time(e), device="cuda")
+    e2e_value = ndist.weak_scaling_rate(n * args.steps, world, e2e_ms * 1e-3) / 1e6
 
     # precision stress (7x7 rational patches, extreme weights, collapsed edges, 25% grazing rays):
     # throughput and the share of FP64 work; its errors against the FP64 oracle are checked by
@@ -494,8 +478,7 @@ def nrt_arm(args):
                 "gpu_launches": args.steps * cnt["kernel_launches"], "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     scene.close()
-    if world > 1:
-        dist.destroy_process_group()
+    ndist.finalize()
 
 
 def main():
