@@ -211,13 +211,16 @@ typedef struct {
     int32_t graph;           /* 1: rounds run inside one CUDA graph with a device-side loop (no host
                                 synchronisation); 2: host-driven rounds (one synchronisation each) */
     int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 530 bytes per ray) */
+    int32_t quota0;          /* candidates a ray emits in the first round, doubling per round ... */
+    int32_t quota_max;       /* ... up to this many (<= 8); the default 4, then 8 */
 } nrt_wavefront_tuning;
 int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out);
 int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in);
 /* Autotuner: times nrt_intersect (wavefront) on these rays and buffers under
  * candidate launch shapes, one knob at a time (coordinate descent over
- * traversal and scatter grids, class-launch blocks and rays per pass; the
- * graph/host-driven choice stays as set), and keeps the fastest on the scene.  *out gets it and
+ * traversal and scatter grids, class-launch blocks, round quotas and rays
+ * per pass; the graph/host-driven choice stays as set), and keeps the
+ * fastest on the scene.  *out gets it and
  * *best_ms its time per call (CUDA events, `reps` calls after one untimed
  * call).  Synchronous.  Results do not depend on the tuning. */
 int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
@@ -266,9 +269,13 @@ int nrt_generate_camera_rays(const nrt_camera* cam, const nrt_rays_out* out, voi
  * cosine-weighted direction about it from a PCG hash of (seed, ray index),
  * and the origin S + offset * normal.  hits->geom is required.  The output is
  * compacted in ray order: out[k], k < *n_out, with src_index[k] the input
- * ray.  Synchronises `stream` (to return *n_out). */
+ * ray.  scratch: device memory of nrt_bounce_scratch_bytes(n) bytes, or NULL
+ * to let the call allocate and free it.  Synchronises `stream` (to return
+ * *n_out). */
+size_t nrt_bounce_scratch_bytes(int64_t n);
 int nrt_generate_bounce_rays(const nrt_rays* rays, const nrt_hits* hits, int64_t n, uint32_t seed, float offset,
-                             const nrt_rays_out* out, int32_t* src_index, int64_t* n_out, void* stream);
+                             const nrt_rays_out* out, int32_t* src_index, int64_t* n_out, void* scratch,
+                             void* stream);
 
 /* ------------------------------------------------------------------------
  * Learned initial guess (no reference counterpart: the reference starts every

@@ -753,7 +753,8 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
                 e = dev::launch_wavefront(scene->view, scene->plan, rc, m, dc, hc, wb, scene->host_count,
                                           scene->counters, st, &scene->last_launches, &scene->last_rounds,
                                           scene->timing_on ? scene->tev : nullptr,
-                                          scene->timing_on ? &scene->newton_ms : nullptr, &scene->newton_launches);
+                                          scene->timing_on ? &scene->newton_ms : nullptr, &scene->newton_launches,
+                                          scene->tuning.quota0, scene->tuning.quota_max);
             }
             if (prev != scene->device) cudaSetDevice(prev);
             if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
@@ -798,6 +799,8 @@ int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out) {
     out->class_blocks = scene->tuning.class_blocks > 0 ? scene->tuning.class_blocks : (int32_t)scene->plan.class_grid[0];
     out->graph = scene->use_graph ? 1 : 2;
     out->chunk = scene->wf_chunk;
+    out->quota0 = scene->tuning.quota0;
+    out->quota_max = scene->tuning.quota_max;
     return NRT_OK;
 }
 
@@ -807,11 +810,17 @@ int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in) {
         return fail(NRT_ERR_INVALID, "block counts above 2^24");
     if (in->graph > 2) return fail(NRT_ERR_INVALID, "graph must be 1 (graph) or 2 (host-driven)");
     if (in->chunk > (1LL << 30)) return fail(NRT_ERR_INVALID, "chunk above 2^30 rays");
+    if (in->quota0 > 8 || in->quota_max > 8) return fail(NRT_ERR_INVALID, "round quotas above 8");
+    const int q0 = in->quota0 > 0 ? in->quota0 : scene->tuning.quota0;
+    const int qm = in->quota_max > 0 ? in->quota_max : scene->tuning.quota_max;
+    if (q0 > qm) return fail(NRT_ERR_INVALID, "quota0 %d above quota_max %d", q0, qm);
     if (in->step_blocks > 0) scene->tuning.step_blocks = in->step_blocks;
     if (in->scatter_blocks > 0) scene->tuning.scatter_blocks = in->scatter_blocks;
     if (in->class_blocks > 0) scene->tuning.class_blocks = in->class_blocks;
     if (in->graph > 0) scene->use_graph = in->graph == 1;
     if (in->chunk > 0) scene->wf_chunk = in->chunk;  // the scratch is re-carved on the next call
+    scene->tuning.quota0 = q0;
+    scene->tuning.quota_max = qm;
     return NRT_OK;
 }
 
@@ -855,6 +864,7 @@ int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_in
     const int64_t scats[] = {148 * 4, 148 * 8, 148 * 16, 148 * 64};
     const int32_t classes[] = {148 * 2, 148 * 4, 148 * 8, 148 * 16};
     const int64_t chunks[] = {1LL << 21, 1LL << 22, 1LL << 23};
+    const int32_t quotas[] = {1 << 8 | 8, 2 << 8 | 8, 4 << 8 | 8, 1 << 8 | 4};  // (first round, cap)
     for (int pass = 0; pass < 2 && status == NRT_OK; ++pass) {
         auto knob = [&](auto&& values, int count, auto&& set) {
             for (int k = 0; k < count && status == NRT_OK; ++k) {
@@ -881,6 +891,13 @@ int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_in
         knob(classes, 4, [&](nrt_wavefront_tuning& t, int32_t v) {
             if (v == t.class_blocks) return false;
             t.class_blocks = v;
+            return true;
+        });
+        knob(quotas, 4, [&](nrt_wavefront_tuning& t, int32_t v) {
+            const int q0 = v >> 8, qm = v & 255;
+            if (q0 == t.quota0 && qm == t.quota_max) return false;
+            t.quota0 = q0;
+            t.quota_max = qm;
             return true;
         });
         knob(chunks, 3, [&](nrt_wavefront_tuning& t, int64_t v) {
@@ -949,8 +966,11 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
     return NRT_OK;
 }
 
+size_t nrt_bounce_scratch_bytes(int64_t n) { return n > 0 ? (size_t)((n + 255) / 256 + 1) * sizeof(int32_t) : 0; }
+
 int nrt_generate_bounce_rays(const nrt_rays* rays, const nrt_hits* hits, int64_t n, uint32_t seed, float offset,
-                             const nrt_rays_out* out, int32_t* src_index, int64_t* n_out, void* stream) {
+                             const nrt_rays_out* out, int32_t* src_index, int64_t* n_out, void* user_scratch,
+                             void* stream) {
     if (!rays || !hits || !out || !src_index || !n_out) return fail(NRT_ERR_INVALID, "null argument");
     if (!hits->patch || !hits->geom) return fail(NRT_ERR_INVALID, "bounce rays need hits->patch and hits->geom");
     if (!out->ox || !out->oy || !out->oz || !out->dx || !out->dy || !out->dz || !rays->dx || !rays->dy || !rays->dz)
@@ -960,16 +980,18 @@ int nrt_generate_bounce_rays(const nrt_rays* rays, const nrt_hits* hits, int64_t
     if (n == 0) return NRT_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long nb = (n + 255) / 256;
-    int32_t* scratch = nullptr;
-    NRT_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&scratch), (nb + 1) * sizeof(int32_t), st), "cudaMallocAsync");
+    int32_t* scratch = static_cast<int32_t*>(user_scratch);
+    if (!scratch) NRT_CUDA(cudaMalloc(reinterpret_cast<void**>(&scratch), (nb + 1) * sizeof(int32_t)), "cudaMalloc");
     const nrt::dev::Rays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz};
     cudaError_t e = nrt::dev::launch_bounce_rays(r, hits->patch, hits->geom, n, seed, offset, out->ox, out->oy, out->oz,
                                                  out->dx, out->dy, out->dz, src_index, scratch, st);
     int32_t total = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&total, scratch + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-    const cudaError_t ef = cudaFreeAsync(scratch, st);
-    if (e == cudaSuccess) e = ef;
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (!user_scratch) {
+        const cudaError_t ef = cudaFree(scratch);
+        if (e == cudaSuccess) e = ef;
+    }
     if (e != cudaSuccess) return cuda_fail(e, "bounce rays");
     *n_out = total;
     return NRT_OK;

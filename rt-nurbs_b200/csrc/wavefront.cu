@@ -9,7 +9,7 @@
 //                    stack, pruning every entry whose box entry is not nearer
 //                    than the ray's best hit so far (the reference's rule,
 //                    src/gpu/intersect.cu:169-183), and emits the leaf patches
-//                    it reaches, up to round_quota(r) of them; counts them per
+//                    it reaches, up to the round's quota of them; counts them per
 //                    patch rank; saves the stack; rays with a non-empty stack
 //                    stay active.
 //   k_wf_scan        exclusive scan of the per-rank counts.
@@ -196,11 +196,12 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
 // grid can be sized to the GPU and a round with few active rays costs no
 // empty blocks.
 __global__ void __launch_bounds__(128) k_wf_step_dev(Scene sc, Rays rays, long long n, Opts op, WfBuffers wb,
-                                                     int32_t* tests, unsigned long long* ctr, const int32_t* rank_of) {
+                                                     int32_t* tests, unsigned long long* ctr, const int32_t* rank_of,
+                                                     int quota0, int quota_max) {
     __shared__ int s_base;
     const int round = wb.counts[2], cur = round & 1;
     const int n_active = round == 0 ? (int)n : wb.counts[cur];
-    const int quota = round_quota(round);
+    const int quota = round_quota(round, quota0, quota_max);
     StepTally c{};
     unsigned long long seen = 0;
     for (;;) {
@@ -398,7 +399,7 @@ static void wf_resolve_class(int p, int q, const WfClassLaunch& L) {
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds, cudaEvent_t* ev,
-                             double* newton_ms, long long* newton_launches) {
+                             double* newton_ms, long long* newton_launches, int quota0, int quota_max) {
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     int n_active = (int)n, cur = 0;
@@ -412,7 +413,8 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         if (e == cudaSuccess) e = cudaMemsetAsync(wb.counts + (1 - cur), 0, sizeof(int), stream);
         if (e != cudaSuccess) return e;
         k_wf_step<<<(unsigned)((n_active + 127) / 128), 128, 0, stream>>>(sc, rays, n, round, n_active,
-                                                                         round_quota(round), op, wb, cur, out.tests,
+                                                                         round_quota(round, quota0, quota_max), op, wb,
+                                                                         cur, out.tests,
                                                                          ctr, plan.rank_of);
         k_wf_scan<<<1, 1024, 0, stream>>>(plan.n_slots, wb);
         k_wf_scatter<<<(unsigned)((n_active + 255) / 256), 256, 0, stream>>>(rays, round, n_active, wb, cur,
@@ -528,7 +530,8 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
             if (e == cudaSuccess) {
                 const unsigned step_grid = (unsigned)std::max(1LL, std::min<long long>((m + 127) / 128, tu.step_blocks));
                 const unsigned scat_grid = (unsigned)std::max(1LL, std::min<long long>((m + 255) / 256, tu.scatter_blocks));
-                k_wf_step_dev<<<step_grid, 128, 0, cs>>>(sc, rc, m, oc, wb, hc.tests, ctr, plan.rank_of);
+                k_wf_step_dev<<<step_grid, 128, 0, cs>>>(sc, rc, m, oc, wb, hc.tests, ctr, plan.rank_of, tu.quota0,
+                                                         tu.quota_max);
                 k_wf_scan<<<1, 1024, 0, cs>>>(plan.n_slots, wb);
                 k_wf_scatter_dev<<<scat_grid, 256, 0, cs>>>(rc, m, wb, plan.rank_of);
                 for (int c = 0; c < plan.n_classes; ++c) {

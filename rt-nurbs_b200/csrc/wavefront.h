@@ -20,8 +20,13 @@ struct __align__(16) WfItem {
 };
 constexpr unsigned long long kNoHit = ~0ull;
 
-// Candidates per ray in round r: 1, 2, 4, then 8.
-__host__ __device__ constexpr int round_quota(int r) { return r >= 3 ? 8 : (1 << r); }
+// Candidates per ray in round r: q0, 2 q0, 4 q0, ... up to qmax (the
+// launch-shape default is 4, then 8; the noalloc and collection paths use
+// 1, 2, 4, 8).  qmax <= 8 keeps a round's emissions (quota plus the rest
+// of one leaf of <= 8 patches) within kEmitMax.
+__host__ __device__ constexpr int round_quota(int r, int q0 = 1, int qmax = 8) {
+    return r >= 4 ? qmax : ((q0 << r) < qmax ? (q0 << r) : qmax);
+}
 
 // Scratch of one wavefront launch over n rays (device pointers).
 struct WfBuffers {
@@ -98,6 +103,8 @@ struct WfTuning {
     long long step_blocks = 148 * 8;     // persistent k_wf_step_dev blocks of 128 (capped at one ray per thread)
     long long scatter_blocks = 148 * 8;  // persistent k_wf_scatter_dev blocks of 256 (same)
     int class_blocks = 0;               // k_wf_newton blocks of 256 per class launch; 0 = the plan's
+    int quota0 = 4;                     // candidates per ray in the first round (doubling each round)
+    int quota_max = 8;                  // ... up to this many (<= 8)
 };
 
 // The whole intersection of n rays as one executable CUDA graph, in passes of
@@ -119,7 +126,8 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds,
-                             cudaEvent_t* ev = nullptr, double* newton_ms = nullptr, long long* newton_launches = nullptr);
+                             cudaEvent_t* ev = nullptr, double* newton_ms = nullptr, long long* newton_launches = nullptr,
+                             int quota0 = 1, int quota_max = 8);
 
 // Per-pixel kernel over a device list of ray indices (count read on the device).
 cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const int32_t* list,

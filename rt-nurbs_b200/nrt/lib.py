@@ -83,7 +83,7 @@ class Counters(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("step_blocks", C.c_int64), ("scatter_blocks", C.c_int64), ("class_blocks", C.c_int32),
-                ("graph", C.c_int32), ("chunk", C.c_int64)]
+                ("graph", C.c_int32), ("chunk", C.c_int64), ("quota0", C.c_int32), ("quota_max", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -136,8 +136,10 @@ def lib():
                                    C.POINTER(Tuning), C.POINTER(C.c_float), vp]
         L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
         L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
+        L.nrt_bounce_scratch_bytes.argtypes = [C.c_int64]
+        L.nrt_bounce_scratch_bytes.restype = C.c_size_t
         L.nrt_generate_bounce_rays.argtypes = [C.POINTER(RaysC), C.POINTER(HitsC), C.c_int64, C.c_uint32, C.c_float,
-                                               C.POINTER(RaysC), vp, C.POINTER(C.c_int64), vp]
+                                               C.POINTER(RaysC), vp, C.POINTER(C.c_int64), vp, vp]
         L.nrt_mlp_param_count.restype = C.c_size_t
         L.nrt_mlp_create.argtypes = [C.c_int, C.c_uint32, C.POINTER(vp)]
         L.nrt_mlp_destroy.argtypes = [vp]
@@ -380,12 +382,13 @@ def bounce_rays(rays, hits, seed=0, offset=1e-4, out=None, stream=None):
         src = torch.empty(n, dtype=torch.int32, device=dev)
     else:
         out, src = out
+    scratch = torch.empty(max(1, int(lib().nrt_bounce_scratch_bytes(n))), dtype=torch.uint8, device=dev)
     r = RaysC(*[C.c_void_p(a.data_ptr()) for a in rays])
     h = HitsC(_ptr(hits["patch"]), _ptr(hits["t"]), _ptr(hits["u"]), _ptr(hits["v"]), None, None, _ptr(hits["geom"]))
     o = RaysC(*[C.c_void_p(a.data_ptr()) for a in out])
     m = C.c_int64()
     _check(lib().nrt_generate_bounce_rays(C.byref(r), C.byref(h), n, int(seed) & 0xFFFFFFFF, float(offset), C.byref(o),
-                                          _ptr(src), C.byref(m), _stream_ptr(stream)))
+                                          _ptr(src), C.byref(m), _ptr(scratch), _stream_ptr(stream)))
     k = int(m.value)
     return [a[:k] for a in out], src[:k], k
 

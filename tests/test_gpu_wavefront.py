@@ -145,14 +145,17 @@ def test_tuning_changes_nothing_and_autotune(nrt_gpu):
     c0 = scene.counters()
     assert c0["rounds"] > 1 and c0["kernel_launches"] > c0["rounds"]
     for kw in [dict(graph=2), dict(graph=1, step_blocks=37, scatter_blocks=11, class_blocks=5),
-               dict(graph=1, chunk=10007), dict(graph=2, chunk=4096)]:
+               dict(graph=1, chunk=10007), dict(graph=2, chunk=4096), dict(graph=1, quota0=8, quota_max=8),
+               dict(graph=2, quota0=1, quota_max=1), dict(graph=1, quota0=2, quota_max=4)]:
         scene.set_tuning(**kw)
         b = to_numpy(scene.intersect(rays, opts))
         c = scene.counters()
-        for k in ("patch", "t", "u", "v", "iters", "tests"):
+        for k in ("patch", "t", "u", "v", "iters") + (() if "quota0" in kw else ("tests",)):
             assert np.array_equal(base[k], b[k]), (k, kw)
-        assert c["newton_evals"] == c0["newton_evals"] and c["hits"] == c0["hits"], kw
-    scene.set_tuning(chunk=1 << 23)
+        assert c["hits"] == c0["hits"], kw
+        if "quota0" not in kw:  # the round quotas change which candidates are pruned, not the hits
+            assert c["newton_evals"] == c0["newton_evals"], kw
+    scene.set_tuning(chunk=1 << 23, quota0=1, quota_max=8)
     scene.enable_counters(False)
     t, ms = scene.autotune(rays, opts, reps=1)
     assert ms > 0 and t["graph"] in (1, 2) and t["step_blocks"] > 0
