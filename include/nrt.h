@@ -61,6 +61,21 @@ typedef struct {
 int nrt_decompose_count(const nrt_nurbs_surface* surf, int* nbU, int* nbV);
 int nrt_decompose(const nrt_nurbs_surface* surf, float* cp_out, float* ranges_out, int* nbU, int* nbV);
 
+/* Curvature-driven refinement before decomposition: knots inserted along u,
+ * then along v, as NurbsOps::curvatureRefinementU / curvatureRefinementV
+ * (src/math/nurbs.h:289-486, applied in that order by src/core/main.cpp:100-102).
+ * Each knot span gets floor(C * max|A_j| * span^1.5 / sqrt(mean |V_j|))
+ * evenly spaced knots (NurbsOps::knotsToAdd, src/math/nurbs.h:254-281; V_j and
+ * A_j the first- and second-derivative control vectors of the span,
+ * maximised over the net's lines), inserted by Algorithm A5.1 (float, the
+ * reference's order of operations).  C <= 0 leaves the surface unchanged.
+ * nrt_refine_count gives (n, m) after refinement; nrt_refine_surface writes
+ * the (n+1)*(m+1) points (index i*(m+1)+j) and the n+p+2 and m+q+2 knots.
+ * Host, synchronous. */
+int nrt_refine_count(const nrt_nurbs_surface* surf, float C, int* n_out, int* m_out);
+int nrt_refine_surface(const nrt_nurbs_surface* surf, float C, float* cp_out, float* u_knots_out, float* v_knots_out,
+                       int* n_out, int* m_out);
+
 /* Patch bounding boxes from the dehomogenised control points:
  * BezierPatchOps::bounds (src/math/bezier_patch.h:153-169).  boxes: 6 floats
  * per patch (min xyz, max xyz).  cp_offset[k] is the first point of patch k,

@@ -18,6 +18,7 @@ never calls it.
 from __future__ import annotations
 
 import ctypes as C
+import ctypes as C_
 import os
 import subprocess
 from dataclasses import dataclass
@@ -285,6 +286,26 @@ def patch_eval_f64(cp64: np.ndarray, p: int, q: int, u: float, v: float) -> np.n
 
 # ---------------------------------------------------------------------------
 # The reference's own code (oracle/_ref), for pinning the restatement.
+def ref_refine(surf, C: float, iters: int = 7):
+    """The reference's curvatureRefinementU then V (src/math/nurbs.h:289-486) on a copy
+    of surf: (cp (P,4), U, V, n, m)."""
+    L = ref_lib(iters)
+    L.ref_refine.argtypes = [f32p, f32p, f32p, C_int := C_.c_int, C_int, C_int, C_int, C_.c_float, f32p, f32p, f32p,
+                             C_.c_long, C_int, C_int, C_.POINTER(C_int), C_.POINTER(C_int)]
+    cap_pts, cap_k = 1 << 21, 1 << 16
+    cp = np.zeros((cap_pts, 4), np.float32)
+    U = np.zeros(cap_k, np.float32)
+    V = np.zeros(cap_k, np.float32)
+    n, m = C_.c_int(), C_.c_int()
+    rc = L.ref_refine(np.ascontiguousarray(surf.cp, np.float32), np.ascontiguousarray(surf.U, np.float32),
+                      np.ascontiguousarray(surf.V, np.float32), surf.n, surf.m, surf.p, surf.q, float(C), cp, U, V,
+                      cap_pts, cap_k, cap_k, C_.byref(n), C_.byref(m))
+    if rc != 0:
+        raise RuntimeError(f"ref_refine failed ({rc})")
+    n, m = n.value, m.value
+    return cp[:(n + 1) * (m + 1)].copy(), U[:n + surf.p + 2].copy(), V[:m + surf.q + 2].copy(), n, m
+
+
 def ref_decompose(surf, iters: int = 7):
     L = ref_lib(iters)
     nbU, nbV = C.c_int(), C.c_int()

@@ -33,6 +33,39 @@ extern "C" {
 
 int ref_iterations(void) { return NEWTON_MAX_ITERATIONS; }
 
+// curvatureRefinementU then curvatureRefinementV (src/math/nurbs.h:289-486) on
+// a copy of the surface, as src/core/main.cpp:100-102.  Writes the refined
+// points and knots when they fit the capacities (points, u knots, v knots);
+// returns 0, -1 when the V pass would overrun the reference's own scratch
+// (it sizes a curve by n+1 and fills m+1 points), -2 when the outputs do not fit.
+int ref_refine(const float* cp, const float* U, const float* V, int n, int m, int p, int q, float C, float* cp_out,
+               float* U_out, float* V_out, long cap_pts, int cap_u, int cap_v, int* n_out, int* m_out) {
+    float* Uk = new float[n + p + 2];
+    float* Vk = new float[m + q + 2];
+    vector4f* P = new vector4f[(size_t)(n + 1) * (m + 1)];
+    std::memcpy(Uk, U, sizeof(float) * (n + p + 2));
+    std::memcpy(Vk, V, sizeof(float) * (m + q + 2));
+    std::memcpy(P, cp, sizeof(vector4f) * (size_t)(n + 1) * (m + 1));
+    NurbsOps::curvatureRefinementU(Uk, p, n, m, C, P);
+    int rc = 0;
+    if (m > n) rc = -1;
+    else NurbsOps::curvatureRefinementV(Vk, q, m, n, C, P);
+    if (rc == 0) {
+        *n_out = n;
+        *m_out = m;
+        if ((long)(n + 1) * (m + 1) > cap_pts || n + p + 2 > cap_u || m + q + 2 > cap_v) rc = -2;
+        else {
+            std::memcpy(cp_out, P, sizeof(vector4f) * (size_t)(n + 1) * (m + 1));
+            std::memcpy(U_out, Uk, sizeof(float) * (n + p + 2));
+            std::memcpy(V_out, Vk, sizeof(float) * (m + q + 2));
+        }
+    }
+    delete[] Uk;
+    delete[] Vk;
+    delete[] P;
+    return rc;
+}
+
 // getPatch on one surface; cp_out gets nbU*nbV*(p+1)*(q+1) points, ranges 4 floats per patch.
 int ref_decompose(const float* cp, const float* U, const float* V, int n, int m, int p, int q, float* cp_out,
                   float* ranges) {

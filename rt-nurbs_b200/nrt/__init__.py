@@ -23,6 +23,7 @@ from .lib import (  # noqa: F401
     lib_path,
     patch_bounds,
     reference_opts,
+    refine,
     INIT_BILINEAR,
     INIT_LEARNED,
     INIT_MIDPOINT,

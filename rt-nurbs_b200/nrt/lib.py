@@ -136,6 +136,9 @@ def lib():
                                    C.POINTER(Tuning), C.POINTER(C.c_float), vp]
         L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
         L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
+        L.nrt_refine_count.argtypes = [C.POINTER(NurbsSurface), C.c_float, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.nrt_refine_surface.argtypes = [C.POINTER(NurbsSurface), C.c_float, vp, vp, vp, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]
         L.nrt_bounce_scratch_bytes.argtypes = [C.c_int64]
         L.nrt_bounce_scratch_bytes.restype = C.c_size_t
         L.nrt_generate_bounce_rays.argtypes = [C.POINTER(RaysC), C.POINTER(HitsC), C.c_int64, C.c_uint32, C.c_float,
@@ -186,6 +189,23 @@ def _surface_struct(s):
     V = np.ascontiguousarray(s.V, np.float32)
     st = NurbsSurface(cp.ctypes.data, U.ctypes.data, V.ctypes.data, s.n, s.m, s.p, s.q)
     return st, (cp, U, V)
+
+
+def refine(s, c: float):
+    """nrt_refine_surface: the surface after curvature-driven knot insertion with
+    constant c (a scenes.Surface)."""
+    from .scenes import Surface
+
+    L = lib()
+    st, keep = _surface_struct(s)
+    n, m = C.c_int(), C.c_int()
+    _check(L.nrt_refine_count(C.byref(st), float(c), C.byref(n), C.byref(m)))
+    cp = np.zeros(((n.value + 1) * (m.value + 1), 4), np.float32)
+    U = np.zeros(n.value + s.p + 2, np.float32)
+    V = np.zeros(m.value + s.q + 2, np.float32)
+    _check(L.nrt_refine_surface(C.byref(st), float(c), cp.ctypes.data, U.ctypes.data, V.ctypes.data, C.byref(n),
+                                C.byref(m)))
+    return Surface(cp, U, V, n.value, m.value, s.p, s.q)
 
 
 def decompose(s):

@@ -80,6 +80,31 @@ def main():
     fixture(scenes.analytic_scene("torus", 96, 54), "torus")
     fixture(scenes.analytic_scene("sphere", 96, 54), "sphere")
     fixture(small_mixed_scene(), "mixed4")
+    refine_fixture()
+
+
+def refine_surfaces():
+    """Surfaces and refinement constants of the refinement fixture: the exact
+    torus and sphere at the reference's own sweep values, the height field, and
+    one random mixed-degree surface with fewer v than u points."""
+    rnd = scenes.random_surface(np.random.default_rng(4), (0.0, 0.0, 0.0), (2, 5), (9, 12), 0.4)
+    return [("torus", scenes.torus_surface(), (1.0, 4.0, 16.0)), ("sphere", scenes.sphere_surface(), (2.0, 8.0)),
+            ("heightfield", scenes.heightfield_scene(0).surfaces[0], (2.0, 4.0)), ("random", rnd, (4.0,))]
+
+
+def refine_fixture():
+    """The reference's curvature refinement (curvatureRefinementU then V) of each
+    surface at each constant: refine.npz."""
+    rec = {}
+    for name, s, cs in refine_surfaces():
+        rec[f"{name}_cp"], rec[f"{name}_U"], rec[f"{name}_V"] = s.cp, s.U, s.V
+        rec[f"{name}_nmpq"] = np.array([s.n, s.m, s.p, s.q], np.int32)
+        rec[f"{name}_C"] = np.array(cs, np.float32)
+        for c in cs:
+            cp, U, V, n, m = O.ref_refine(s, c)
+            rec[f"{name}_C{c:g}_cp"], rec[f"{name}_C{c:g}_U"], rec[f"{name}_C{c:g}_V"] = cp, U, V
+            rec[f"{name}_C{c:g}_nm"] = np.array([n, m], np.int32)
+    np.savez_compressed(os.path.join(OUT, "refine.npz"), **rec)
 
 
 if __name__ == "__main__":

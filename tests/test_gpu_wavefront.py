@@ -163,3 +163,25 @@ def test_tuning_changes_nothing_and_autotune(nrt_gpu):
     b = to_numpy(scene.intersect(rays, opts))
     for k in ("patch", "t", "u", "v", "iters"):
         assert np.array_equal(base[k], b[k]), k
+
+
+def test_refined_torus(nrt_gpu, oracle_mod):
+    """The exact torus after the reference's curvature refinement (C = 4, as
+    src/core/main.cpp:100-102): both schedules agree with each other and with
+    the FP64 oracle on the refined patches."""
+    from nrt import scenes
+
+    sc = scenes.analytic_scene("torus", 192, 108)
+    surf = nrt_gpu.refine(sc.surfaces[0], 4.0)
+    scene = nrt_gpu.Scene([surf])
+    rays = nrt_gpu.camera_rays(sc.camera)
+    opts = nrt_gpu.default_opts(hull_cull=3, fp64_final=1, cond_fp64=1e4, schedule=nrt_gpu.SCHED_WAVEFRONT)
+    out = to_numpy(scene.intersect(rays, opts))
+    same_as_pixel(nrt_gpu, scene, rays, opts.replace(hull_cull=1))
+    P = oracle_mod.decompose_scene([surf], f64=False)
+    P.cp64 = P.cp.astype(np.float64)
+    ref = oracle_mod.intersect(P, oracle_mod.build_bvh(oracle_mod.patch_boxes(P)),
+                               oracle_mod.Rays(*[a.cpu().numpy() for a in rays]), 0, 8, 1e-6, f64=True)
+    st = compare(out, ref.patch, ref.t, ref.u, ref.v)
+    assert st["hit_rate"] > 0.05 and st["agree"] >= 0.9999, st
+    assert st["t_rel_max"] <= 1e-4, st
