@@ -179,7 +179,9 @@ typedef struct {
                              split at u = 1/2, or at v = 1/2 */
     int schedule;         /* NRT_SCHED_PIXEL or NRT_SCHED_WAVEFRONT */
     int seed_offset;      /* added to the ray index to seed the singular-Jacobian pull */
-    float flat_threshold; /* flat-skip in pixels (src/gpu/intersect.cu:104-123); 0 = off */
+    float flat_threshold; /* flat-skip in pixels (src/gpu/intersect.cu:104-123); 0 = off.  Both
+                             schedules; the culls (hull_cull) can remove pairs that flat-skip
+                             would accept, as the reference has no cull */
     float cam_k;          /* 0.5*H/tan(vfov/2), only used by flat-skip */
     int learned_iters;    /* NRT_INIT_LEARNED: evaluations from the network's guess before
                              falling back to plain Newton from (0.5,0.5); 0 = max_iter */
@@ -254,6 +256,8 @@ typedef struct {
     double newton_kernel_ms;           /* with kernel timing on: device time of the per-class Newton
                                           launches of the last nrt_intersect (CUDA events) */
     uint64_t newton_kernel_launches;   /* with kernel timing on: how many such launches */
+    uint64_t flat_skips;               /* (ray, patch) tests accepted by flat-skip without Newton
+                                          (the reference's skip_count, src/gpu/intersect.cu:111) */
 } nrt_counters;
 int nrt_enable_counters(nrt_scene* scene, int enable);
 /* Kernel timing for roofline measurement: while enabled, the wavefront runs

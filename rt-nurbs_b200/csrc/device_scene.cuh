@@ -24,6 +24,8 @@ struct Scene {
     const float* delta;      // per slot: flatness (patchDelta) for flat-skip
     const PatchFrame* frames;  // per slot: frame of the learned guess's features
     const float4* obb;       // per slot: oriented box of the control points, 4 float4 (see obb_misses)
+    const float4* leafbox;   // per slot: the box of its BVH leaf (lo xyz, hi xyz in two float4), as the
+                             // parent node stores it (the flat-skip's entry distance)
     int n_slots;
 };
 
@@ -55,10 +57,39 @@ struct Opts {
     long long col_cap;
 };
 
+// Flat-skip (src/gpu/intersect.cu:104-123): when the patch's projected
+// flatness delta * cam_k / te (te: the ray's entry distance into the leaf box)
+// is below the pixel threshold, the patch is evaluated at the initial guess
+// and the guess is accepted when its projected plane residual is below the
+// threshold too.  Returns true with o holding the point (evals 0, flat 1);
+// the caller still requires 0 < t (and t below its best hit).
+template <int P, int Q>
+__device__ __forceinline__ bool flat_accept(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                            float delta, float te, const Opts& op, float gu, float gv, NewtonOut& o) {
+    if (!(op.flat_threshold > 0.f && delta * op.cam_k / te < op.flat_threshold)) return false;
+    float H[4], Hu[4], Hv[4];
+    eval_patch<P, Q, float>(blk, gu, gv, H, Hu, Hv);
+    const float iw = __frcp_rn(H[3]);
+    const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
+    const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
+    const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
+    if (!((fabsf(r1) + fabsf(r2)) * op.cam_k / te < op.flat_threshold)) return false;
+    o.evals = 0;
+    o.u = gu; o.v = gv;
+    o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
+    o.sx = sx; o.sy = sy; o.sz = sz;
+    o.ux = (Hu[0] - sx * Hu[3]) * iw; o.uy = (Hu[1] - sy * Hu[3]) * iw; o.uz = (Hu[2] - sz * Hu[3]) * iw;
+    o.vx = (Hv[0] - sx * Hv[3]) * iw; o.vy = (Hv[1] - sy * Hv[3]) * iw; o.vz = (Hv[2] - sz * Hv[3]) * iw;
+    o.fp64_solves = 0;
+    o.fp64_final = 0;
+    o.flat = 1;
+    return true;
+}
+
 // Indices into the device counter block (nrt_counters order).
 enum Counter : int {
     kRays = 0, kBoxTests, kCandidates, kCulled, kSolves, kEvals, kFp64Solves, kFp64Final, kHits, kErrors, kLearned,
-    kFallbacks, kRoundsDone, kNumCounters
+    kFallbacks, kRoundsDone, kFlatSkips, kNumCounters
 };
 // Followed by 64 per-degree evaluation counts and 64 per-degree hull-test counts.
 constexpr int kEvalsByDegree = kNumCounters, kHullByDegree = kNumCounters + 64, kCounterWords = kNumCounters + 128;

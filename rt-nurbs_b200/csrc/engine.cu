@@ -329,6 +329,15 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     std::vector<float> delta(N);
     std::vector<dev::PatchFrame> frames(N);
     std::vector<float4> obbs(4 * (size_t)N);
+    // each slot's leaf box as its parent node stores it (the flat-skip's entry distance)
+    std::vector<float4> leafbox(2 * (size_t)N, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (const Node4& nd : wide)
+        for (int c = 0; c < 4; ++c)
+            if (nd.child[c] < 0 && nd.count[c] > 0)
+                for (int k = ~nd.child[c]; k < ~nd.child[c] + nd.count[c]; ++k) {
+                    leafbox[2 * (size_t)k] = make_float4(nd.lo_x[c], nd.lo_y[c], nd.lo_z[c], 0.f);
+                    leafbox[2 * (size_t)k + 1] = make_float4(nd.hi_x[c], nd.hi_y[c], nd.hi_z[c], 0.f);
+                }
     std::vector<float> blocks;
     std::vector<int32_t> slot_patch(N);
     size_t total_floats = 0;
@@ -385,8 +394,9 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
                  sz_cor = align(corners.size() * sizeof(float4)), sz_del = align(N * sizeof(float)),
                  sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long)),
                  sz_rank = align(N * sizeof(int32_t)), sz_frm = align(N * sizeof(dev::PatchFrame)),
-                 sz_obb = align(obbs.size() * sizeof(float4));
-    const size_t total = sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank + sz_frm + sz_obb;
+                 sz_obb = align(obbs.size() * sizeof(float4)), sz_lbx = align(leafbox.size() * sizeof(float4));
+    const size_t total =
+        sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank + sz_frm + sz_obb + sz_lbx;
     // wavefront plan: patches ranked by (p, q, slot); one class per degree pair present
     std::vector<int32_t> by_rank(N), rank_of(N);
     for (int s2 = 0; s2 < N; ++s2) by_rank[s2] = s2;
@@ -434,6 +444,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     plan.rank_of = static_cast<const int32_t*>(put(rank_of.data(), N * sizeof(int32_t), sz_rank));
     sc->view.frames = static_cast<const dev::PatchFrame*>(put(frames.data(), N * sizeof(dev::PatchFrame), sz_frm));
     sc->view.obb = static_cast<const float4*>(put(obbs.data(), obbs.size() * sizeof(float4), sz_obb));
+    sc->view.leafbox = static_cast<const float4*>(put(leafbox.data(), leafbox.size() * sizeof(float4), sz_lbx));
     sc->plan = plan;
     cudaSetDevice(prev);
     if (e != cudaSuccess) {
@@ -669,8 +680,8 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     }
     if (o.schedule != NRT_SCHED_PIXEL && o.schedule != NRT_SCHED_WAVEFRONT)
         return fail(NRT_ERR_INVALID, "unknown schedule %d", o.schedule);
-    if (o.schedule == NRT_SCHED_WAVEFRONT && o.flat_threshold > 0.f)
-        return fail(NRT_ERR_UNSUPPORTED, "flat-skip runs on the per-pixel schedule only");
+    if (o.flat_threshold > 0.f && o.init_mode == NRT_INIT_LEARNED)
+        return fail(NRT_ERR_UNSUPPORTED, "flat-skip tests the midpoint or bilinear guess, not the learned one");
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != scene->device) NRT_CUDA(cudaSetDevice(scene->device), "cudaSetDevice");
@@ -947,6 +958,7 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
     out->errors = h[dev::kErrors];
     out->learned_solves = h[dev::kLearned];
     out->learned_fallbacks = h[dev::kFallbacks];
+    out->flat_skips = h[dev::kFlatSkips];
     if (scene->last_graph) {  // rounds counted on the device; kernels per pass and per round are fixed
         const uint64_t per_pass = 4 + (uint64_t)scene->plan.n_classes, per_round = 4 + (uint64_t)scene->plan.n_classes;
         out->rounds = h[dev::kRoundsDone];

@@ -20,7 +20,7 @@ struct Best {
 };
 
 struct Tally {
-    unsigned long long box, cand, culled, solves, evals, f64s, f64f, err;
+    unsigned long long box, cand, culled, solves, evals, f64s, f64f, err, flat;
 };
 
 template <int P, int Q>
@@ -41,28 +41,12 @@ __device__ __forceinline__ void test_patch(const Scene& sc, int slot, const RayF
     }
     float gu = 0.5f, gv = 0.5f;
     if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
-    if (op.flat_threshold > 0.f && sc.delta[slot] * op.cam_k / te < op.flat_threshold) {
-        // flat-skip (src/gpu/intersect.cu:104-123): accept the guess when its
-        // projected residual is below the pixel threshold
-        float H[4], Hu[4], Hv[4];
-        eval_patch<P, Q, float>(blk, gu, gv, H, Hu, Hv);
-        const float iw = __frcp_rn(H[3]);
-        const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
-        const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
-        const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
-        if ((fabsf(r1) + fabsf(r2)) * op.cam_k / te < op.flat_threshold) {
-            const float t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
-            if (0.f < t && t < b.t_max) {
-                NewtonOut o;
-                o.evals = 0;
-                o.u = gu; o.v = gv; o.t = t;
-                o.sx = sx; o.sy = sy; o.sz = sz;
-                o.ux = (Hu[0] - sx * Hu[3]) * iw; o.uy = (Hu[1] - sy * Hu[3]) * iw; o.uz = (Hu[2] - sz * Hu[3]) * iw;
-                o.vx = (Hv[0] - sx * Hv[3]) * iw; o.vy = (Hv[1] - sy * Hv[3]) * iw; o.vz = (Hv[2] - sz * Hv[3]) * iw;
-                o.fp64_solves = 0; o.fp64_final = 0;
-                b.t_max = t; b.slot = slot; b.o = o;
-                return;
-            }
+    {
+        NewtonOut o;
+        if (flat_accept<P, Q>(blk, r, pr, sc.delta[slot], te, op, gu, gv, o) && 0.f < o.t && o.t < b.t_max) {
+            ++c.flat;
+            b.t_max = o.t; b.slot = slot; b.o = o;
+            return;
         }
     }
     const NewtonOut o = newton<P, Q>(blk, r, pr, gu, gv, seed, op.nw);
@@ -102,7 +86,7 @@ __device__ __forceinline__ void trace_pixel(const Scene& sc, const Rays& rays, l
     Best b;
     b.t_max = INFINITY;
     b.slot = -1;
-    Tally c = {0, 0, 0, 0, 0, 0, 0, 0};
+    Tally c = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int st_ref[kStack];
     float st_t[kStack];
     int sp = 0;
@@ -193,6 +177,7 @@ __device__ __forceinline__ void trace_pixel(const Scene& sc, const Rays& rays, l
         count_add(ctr, kFp64Final, c.f64f);
         count_add(ctr, kHits, b.slot >= 0 ? 1 : 0);
         count_add(ctr, kErrors, c.err);
+        count_add(ctr, kFlatSkips, c.flat);
     } else if (ctr && c.err) {
         atomicAdd(ctr + kErrors, c.err);
     }

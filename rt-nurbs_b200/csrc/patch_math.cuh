@@ -56,6 +56,7 @@ struct NewtonOut {
     float sx, sy, sz, ux, uy, uz, vx, vy, vz;  // S (local), dS/du, dS/dv
     int fp64_solves;
     int fp64_final;
+    int flat;        // 1: accepted by the flat-skip test at the initial guess (evals 0)
 };
 
 // PCG hash (src/math/math_utils.h:12-17).
@@ -595,6 +596,7 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
                                             float u0, float v0, uint32_t seed, const NewtonOpts& op) {
     NewtonOut o;
     o.fp64_solves = 0;
+    o.flat = 0;
     o.fp64_final = 0;
     float u = u0, v = v0;
     for (int it = 1; it <= op.max_iter; ++it) {

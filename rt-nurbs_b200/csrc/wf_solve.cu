@@ -34,7 +34,9 @@ __device__ __forceinline__ void item_ray(const WfItem& it, RayFrame& r) {
 // Newton from (0.5, 0.5) with the full budget, which stays the judge of hits.
 // When the network's raw guess lies outside [-0.25, 1.25]^2 (it predicts no
 // root in the patch) the learned attempt is skipped and plain Newton runs
-// directly.  evals counts both attempts.
+// directly.  evals counts both attempts.  With flat_threshold > 0 (midpoint or
+// bilinear guess) the flat-skip test runs first, as in the per-pixel kernel;
+// an accepted guess comes back with flat = 1 and evals 0.
 template <int P, int Q, bool LEARNED>
 __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const RayFrame& r, const PatchRay& pr,
                                                 const float* __restrict__ blk, float lu, float lv, uint32_t seed,
@@ -55,6 +57,13 @@ __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const
     if (LEARNED) fell_back = 2;  // gated off: plain Newton only
     float gu = 0.5f, gv = 0.5f;
     if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
+    if (!LEARNED && op.flat_threshold > 0.f) {
+        // the ray's entry into the slot's leaf box, computed as the traversal does
+        const float4 lo = __ldg(sc.leafbox + 2 * slot), hi = __ldg(sc.leafbox + 2 * slot + 1);
+        const float te = slab(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, r, __frcp_rn(r.dx), __frcp_rn(r.dy), __frcp_rn(r.dz));
+        NewtonOut o;
+        if (flat_accept<P, Q>(blk, r, pr, __ldg(sc.delta + slot), te, op, gu, gv, o) && 0.f < o.t) return o;
+    }
     return newton<P, Q>(blk, r, pr, gu, gv, seed, nw);
 }
 
@@ -86,7 +95,8 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* qu = queue[warp];
     const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
-    unsigned long long solves = 0, evals = 0, f64 = 0, culled = 0, hull_tests = 0, learned = 0, fallbacks = 0;
+    unsigned long long solves = 0, evals = 0, f64 = 0, culled = 0, hull_tests = 0, learned = 0, fallbacks = 0,
+                       flats = 0;
     NewtonOpts nw = op.nw;
     nw.fp64_final = 0;  // applied to the winner only, in k_wf_resolve
     const float cull_eps = op.nw.eps;
@@ -164,7 +174,8 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
             evals += (unsigned long long)(o.evals > 0 ? o.evals : -o.evals);
             f64 += (unsigned long long)o.fp64_solves;
             if (tests) atomicAdd(tests + it.ray, 1);
-            if (o.evals > 0 && o.t > 0.f) {
+            flats += (unsigned long long)o.flat;
+            if ((o.evals > 0 || o.flat) && o.t > 0.f) {
                 const unsigned long long key = ((unsigned long long)__float_as_uint(o.t) << 32) | (unsigned)it.slot;
                 atomicMin(wb.best_key + it.ray, key);
             }
@@ -187,6 +198,7 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
         count_add(ctr, kCulled, culled);
         count_add(ctr, kLearned, learned);
         count_add(ctr, kFallbacks, fallbacks);
+        count_add(ctr, kFlatSkips, flats);
         if (evals) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, evals);
         if (hull_tests) atomicAdd(ctr + kHullByDegree + P * 8 + Q, hull_tests);
     }
@@ -236,7 +248,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
         const NewtonOut o = solve_item<P, Q, LEARNED>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
                                                       (uint32_t)it.ray + op.seed_offset, op, op.nw, fell);
         const long long i = it.ray;
-        if (o.evals > 0 && o.t > 0.f) {
+        if ((o.evals > 0 || o.flat) && o.t > 0.f) {
             ++hits;
             f64f += (unsigned long long)o.fp64_final;
             out.patch[i] = h.z;
@@ -251,7 +263,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
                 g[6] = o.vx; g[7] = o.vy; g[8] = o.vz;
             }
         } else {
-            if (o.evals <= 0) ++err;  // the recomputed winner must converge again
+            if (o.evals <= 0 && !o.flat) ++err;  // the recomputed winner must converge again
             out.patch[i] = -1;
             out.t[i] = -1.f;
             out.u[i] = 0.f;

@@ -68,7 +68,8 @@ class Counters(C.Structure):
                                                             ("hull_tests_by_degree", C.c_uint64 * 64),
                                                             ("kernel_launches", C.c_uint64), ("rounds", C.c_uint64),
                                                             ("newton_kernel_ms", C.c_double),
-                                                            ("newton_kernel_launches", C.c_uint64)]
+                                                            ("newton_kernel_launches", C.c_uint64),
+                                                            ("flat_skips", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: int(getattr(self, k)) for k in _COUNTER_NAMES}
@@ -78,6 +79,7 @@ class Counters(C.Structure):
         d["rounds"] = int(self.rounds)
         d["newton_kernel_ms"] = float(self.newton_kernel_ms)
         d["newton_kernel_launches"] = int(self.newton_kernel_launches)
+        d["flat_skips"] = int(self.flat_skips)
         return d
 
 

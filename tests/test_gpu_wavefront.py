@@ -183,5 +183,44 @@ def test_refined_torus(nrt_gpu, oracle_mod):
     ref = oracle_mod.intersect(P, oracle_mod.build_bvh(oracle_mod.patch_boxes(P)),
                                oracle_mod.Rays(*[a.cpu().numpy() for a in rays]), 0, 8, 1e-6, f64=True)
     st = compare(out, ref.patch, ref.t, ref.u, ref.v)
-    assert st["hit_rate"] > 0.05 and st["agree"] >= 0.9999, st
+    assert st["hit_rate"] > 0.02 and st["agree"] >= 0.9999, st
     assert st["t_rel_max"] <= 1e-4, st
+
+
+@pytest.mark.parametrize("name", ["heightfield", "torus", "sphere", "mixed4"])
+def test_flat_skip_both_schedules(nrt_gpu, name):
+    """Flat-skip at 2 px with the reference's settings (golden fixture flat2px,
+    made by the reference's own code): the per-pixel kernel and the wavefront
+    agree with each other (the wavefront accepts a flat guess even when a
+    nearer hit is already known, where the per-pixel kernel would run Newton
+    on that patch; both keep the nearest), and both agree with the reference's
+    outputs on >= 99.9 % of hit/miss decisions, on the patch for >= 99 % of
+    rays both hit, with relative t differences <= 1e-2 at the 99th percentile
+    (an accepted flat guess is a pixel-level approximation; different trees
+    and visiting orders accept different guesses)."""
+    g = load_golden(name)
+    scene = nrt_gpu.Scene(golden_surfaces(g))
+    rays = gpu_rays(golden_rays(g))
+    c = g["camera"]
+    cam_k = float(0.5 * c[11] / np.tan(np.radians(c[9]) / 2.0))
+    base = nrt_gpu.reference_opts(flat_threshold=2.0, cam_k=cam_k)
+    scene.enable_counters(True)
+    a = to_numpy(scene.intersect(rays, base))
+    skips_pixel = scene.counters()["flat_skips"]
+    b = to_numpy(scene.intersect(rays, base.replace(schedule=nrt_gpu.SCHED_WAVEFRONT)))
+    skips_wf = scene.counters()["flat_skips"]
+    scene.enable_counters(False)
+    if name in ("heightfield", "mixed4"):  # the torus and sphere fixtures are not flat enough at 2 px
+        assert skips_pixel > 0 and skips_wf > 0
+    hit_a, hit_b = a["patch"] >= 0, b["patch"] >= 0
+    assert (hit_a == hit_b).mean() >= 0.999
+    slot = g["flat2px_hit_slot"]
+    order = g["bvh_order"]
+    ref_patch = np.where(slot >= 0, order[np.maximum(slot, 0)], -1)
+    for out in (a, b):
+        st = compare(out, ref_patch, g["flat2px_t"].astype(np.float64))
+        both = (out["patch"] >= 0) & (ref_patch >= 0)
+        rel = np.abs(out["t"][both] - g["flat2px_t"][both]) / np.abs(g["flat2px_t"][both])
+        print(name, st["agree"], st["same_patch"], np.quantile(rel, 0.99) if rel.size else None)
+        assert st["agree"] >= 0.999 and st["same_patch"] >= 0.99, st
+        assert rel.size == 0 or np.quantile(rel, 0.99) <= 1e-2
