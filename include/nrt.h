@@ -297,6 +297,23 @@ int nrt_generate_bounce_rays(const nrt_rays* rays, const nrt_hits* hits, int64_t
                              void* stream);
 
 /* ------------------------------------------------------------------------
+ * Output stage (headless).  nrt_shade fills a float RGB framebuffer (SoA,
+ * SoAQueue::frame_buffer, src/gpu/soa.h:22-26) from hits: mode 0 the hit mask
+ * in red (redTestShading, src/gpu/testShading.cu:9-24), mode 1 the normal map
+ * (n + 1) / 2 with n = normalize(dS/dv x dS/du) (normalsTestShading,
+ * src/gpu/testShading.cu:27-55; needs hits->geom).  nrt_compare_hits gives per
+ * ray, against a reference hit set, the hit-point distance in pixels
+ * |P_ref - P_test| cam_k / t_ref and the normal angle in degrees (NaN unless
+ * both hit) and a hit/miss mismatch flag, the error measures of the
+ * reference's benchmark (src/core/benchmark.cpp:206-222).  Device buffers,
+ * asynchronous.  nrt_write_ppm writes host RGB floats in [0,1] as a binary
+ * PPM (src/core/benchmark.cpp:85-97). */
+int nrt_shade(const nrt_hits* hits, int64_t n, int mode, float* r, float* g, float* b, void* stream);
+int nrt_compare_hits(const nrt_rays* rays, const nrt_hits* ref, const nrt_hits* test, int64_t n, float cam_k,
+                     float* px_err, float* deg_err, int32_t* mismatch, void* stream);
+int nrt_write_ppm(const char* path, int width, int height, const float* r, const float* g, const float* b);
+
+/* ------------------------------------------------------------------------
  * Learned initial guess (no reference counterpart: the reference starts every
  * solve from its bilinear guess, src/gpu/intersect.cu:102).  A 12-64-64-2
  * MLP with SiLU maps (ray, patch) features to a starting (u, v); BF16 tensor

@@ -17,12 +17,15 @@ from .lib import (  # noqa: F401
     bounce_rays,
     build_bvh_binary,
     camera_rays,
+    compare_hits,
     decompose,
     default_opts,
     lib,
     lib_path,
     patch_bounds,
     reference_opts,
+    shade,
+    write_ppm,
     refine,
     INIT_BILINEAR,
     INIT_LEARNED,

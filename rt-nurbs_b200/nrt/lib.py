@@ -138,6 +138,10 @@ def lib():
                                    C.POINTER(Tuning), C.POINTER(C.c_float), vp]
         L.nrt_get_counters.argtypes = [vp, C.POINTER(Counters), vp]
         L.nrt_generate_camera_rays.argtypes = [C.POINTER(CameraC), C.POINTER(RaysC), vp]
+        L.nrt_shade.argtypes = [C.POINTER(HitsC), C.c_int64, C.c_int, vp, vp, vp, vp]
+        L.nrt_compare_hits.argtypes = [C.POINTER(RaysC), C.POINTER(HitsC), C.POINTER(HitsC), C.c_int64, C.c_float, vp,
+                                       vp, vp, vp]
+        L.nrt_write_ppm.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, vp, vp]
         L.nrt_refine_count.argtypes = [C.POINTER(NurbsSurface), C.c_float, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.nrt_refine_surface.argtypes = [C.POINTER(NurbsSurface), C.c_float, vp, vp, vp, C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]
@@ -413,6 +417,43 @@ def bounce_rays(rays, hits, seed=0, offset=1e-4, out=None, stream=None):
                                           _ptr(src), C.byref(m), _ptr(scratch), _stream_ptr(stream)))
     k = int(m.value)
     return [a[:k] for a in out], src[:k], k
+
+
+def _hits_struct(h):
+    return HitsC(_ptr(h["patch"]), _ptr(h["t"]), _ptr(h["u"]), _ptr(h["v"]), _ptr(h.get("iters")),
+                 _ptr(h.get("tests")), _ptr(h.get("geom")))
+
+
+def shade(hits, mode=1, stream=None):
+    """nrt_shade: (r, g, b) float32 CUDA tensors; mode 0 hit mask, 1 normal map."""
+    import torch
+
+    n = hits["patch"].numel()
+    rgb = [torch.empty(n, dtype=torch.float32, device=hits["patch"].device) for _ in range(3)]
+    h = _hits_struct(hits)
+    _check(lib().nrt_shade(C.byref(h), n, int(mode), *[_ptr(a) for a in rgb], _stream_ptr(stream)))
+    return rgb
+
+
+def compare_hits(rays, ref, test, cam_k, stream=None):
+    """nrt_compare_hits: (pixel error, normal angle in degrees, mismatch) CUDA tensors per ray."""
+    import torch
+
+    n = ref["patch"].numel()
+    dev = ref["patch"].device
+    px, deg = torch.empty(n, device=dev), torch.empty(n, device=dev)
+    mm = torch.empty(n, dtype=torch.int32, device=dev)
+    r = RaysC(*[C.c_void_p(a.data_ptr()) for a in rays])
+    a, b = _hits_struct(ref), _hits_struct(test)
+    _check(lib().nrt_compare_hits(C.byref(r), C.byref(a), C.byref(b), n, float(cam_k), _ptr(px), _ptr(deg), _ptr(mm),
+                                  _stream_ptr(stream)))
+    return px, deg, mm
+
+
+def write_ppm(path, width, height, r, g, b):
+    """nrt_write_ppm from host float arrays (numpy) in [0, 1]."""
+    arrs = [np.ascontiguousarray(x, np.float32) for x in (r, g, b)]
+    _check(lib().nrt_write_ppm(str(path).encode(), int(width), int(height), *[a.ctypes.data for a in arrs]))
 
 
 class Camera(CameraC):
