@@ -89,8 +89,11 @@ int nrt_patch_bounds(const float* cp, const int32_t* cp_offset, const int32_t* d
  * way, src/core/bvh.h:167-175).  Arrays hold 2N-1 nodes; *n_nodes gets the
  * number used.  builder NRT_BVH_EXACT_SAH replaces BvhOps::buildBVH
  * (src/core/bvh.h:148-179) node for node (O(N^2) per level, for small N);
- * NRT_BVH_BINNED_SAH is the O(N log N) builder used for scenes. */
-enum { NRT_BVH_BINNED_SAH = 0, NRT_BVH_EXACT_SAH = 1 };
+ * NRT_BVH_BINNED_SAH is the O(N log N) builder used for scenes (32 bins,
+ * stable partition).  NRT_BVH_BINNED_SAH_DEVICE (scenes only) builds the
+ * same tree on the device, together with the decomposition and the packing:
+ * the scene it creates is bit-identical to NRT_BVH_BINNED_SAH's. */
+enum { NRT_BVH_BINNED_SAH = 0, NRT_BVH_EXACT_SAH = 1, NRT_BVH_BINNED_SAH_DEVICE = 2 };
 int nrt_build_bvh_binary(const float* boxes, int n, int builder, float* node_bounds, uint32_t* left_first,
                          uint32_t* prim_count, int32_t* order, int* n_nodes);
 
@@ -104,7 +107,8 @@ int nrt_build_bvh_binary(const float* boxes, int n, int builder, float* node_bou
 typedef struct nrt_scene nrt_scene;
 
 typedef struct {
-    int builder;        /* NRT_BVH_BINNED_SAH (default) or NRT_BVH_EXACT_SAH */
+    int builder;        /* NRT_BVH_BINNED_SAH (default), NRT_BVH_EXACT_SAH, or
+                           NRT_BVH_BINNED_SAH_DEVICE (whole build on the device) */
     int max_leaf;       /* patches per BVH leaf (1..8, default 1) */
     int device;         /* CUDA device ordinal */
     int64_t wavefront_chunk; /* rays per wavefront pass (0 = 2^23); bounds its scratch,
@@ -129,6 +133,10 @@ typedef struct {
 int nrt_scene_get_info(const nrt_scene* scene, nrt_scene_info* info);
 /* Global patch index -> (surface, patch within the surface, u0,u1,v0,v1). Host copies. */
 int nrt_scene_patch_table(const nrt_scene* scene, int32_t* surface_of, float* ranges);
+/* Copies the scene's whole device arena (info.device_bytes bytes: BVH nodes,
+ * packed patches and per-slot tables, counters) to host memory, for
+ * inspection; `bytes` must be at least device_bytes.  Synchronous. */
+int nrt_scene_copy_arena(const nrt_scene* scene, void* host_dst, size_t bytes);
 
 /* ------------------------------------------------------------------------
  * Rays and hits: structure-of-arrays device buffers (SoAQueue::ray_queue,

@@ -8,33 +8,22 @@
 //    scenes.
 //  * build_binned_sah: 32-bin SAH (same cost function), O(N log N), used for
 //    scenes.  Splits until a node holds at most max_leaf patches or its
-//    centroids coincide.
+//    centroids coincide.  The partition is stable, so the tree, its leaf
+//    order and its boxes depend only on the inputs, never on the order in
+//    which nodes are processed: the device builder (scene_build.cu) processes
+//    a level at a time and produces the same tree.
 //  * collapse_to_wide: binary -> 4-wide nodes with SoA child boxes, the layout
-//    the device traverses.
+//    the device traverses, numbered breadth-first (as the device builder
+//    numbers them).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 
-#include "nrt_internal.h"
+#include "scene_math.h"
 
 namespace nrt {
 
 namespace {
-
-inline Box3 empty_box() { return {{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}}; }
-inline Box3 join(const Box3& a, const Box3& b) {
-    Box3 r;
-    for (int k = 0; k < 3; ++k) {
-        r.lo[k] = fminf(a.lo[k], b.lo[k]);
-        r.hi[k] = fmaxf(a.hi[k], b.hi[k]);
-    }
-    return r;
-}
-inline float centre(const Box3& b, int k) { return .5f * (b.lo[k] + b.hi[k]); }
-inline float half_area(const Box3& b) {  // bounds_ops.h:72-77
-    const float ex = b.hi[0] - b.lo[0], ey = b.hi[1] - b.lo[1], ez = b.hi[2] - b.lo[2];
-    return ex * ey + ey * ez + ez * ex;
-}
 
 struct ExactBuilder {
     const std::vector<Box3>& prim;
@@ -110,10 +99,10 @@ void build_exact_sah(const std::vector<Box3>& prims, BinaryBVH& out) {
 void build_binned_sah(const std::vector<Box3>& prims, int max_leaf, BinaryBVH& out) {
     init_out(prims, out);
     if (prims.empty()) return;
-    constexpr int BINS = 32;
     std::vector<float> cen(prims.size() * 3);
     for (size_t i = 0; i < prims.size(); ++i)
         for (int k = 0; k < 3; ++k) cen[3 * i + k] = centre(prims[i], k);
+    SahBins bins;
     // explicit stack instead of recursion (depth is unbounded for bad inputs)
     std::vector<uint32_t> todo{0};
     while (!todo.empty()) {
@@ -127,71 +116,47 @@ void build_binned_sah(const std::vector<Box3>& prims, int max_leaf, BinaryBVH& o
                 clo[k] = fminf(clo[k], cen[3 * out.order[i] + k]);
                 chi[k] = fmaxf(chi[k], cen[3 * out.order[i] + k]);
             }
-        int best_axis = -1, best_split = 0;
-        float best_cost = INFINITY;
+        float ext[3], scale[3];
         for (int a = 0; a < 3; ++a) {
-            const float ext = chi[a] - clo[a];
-            if (!(ext > 0)) continue;
-            Box3 bb[BINS];
-            int bc[BINS] = {0};
-            for (int k = 0; k < BINS; ++k) bb[k] = empty_box();
-            const float scale = BINS / ext;
+            ext[a] = chi[a] - clo[a];
+            scale[a] = kSahBins / ext[a];
+            for (int k = 0; k < kSahBins; ++k) {
+                bins.cnt[a][k] = 0;
+                for (int c = 0; c < 3; ++c) { bins.lo[a][k][c] = INFINITY; bins.hi[a][k][c] = -INFINITY; }
+            }
+            if (!(ext[a] > 0)) continue;
             for (uint32_t i = first; i < first + count; ++i) {
                 const int id = out.order[i];
-                int b = (int)((cen[3 * id + a] - clo[a]) * scale);
-                b = std::min(std::max(b, 0), BINS - 1);
-                ++bc[b];
-                bb[b] = join(bb[b], prims[id]);
-            }
-            float right_area[BINS];
-            int right_count[BINS];
-            Box3 acc = empty_box();
-            int n = 0;
-            for (int k = BINS - 1; k > 0; --k) {
-                acc = join(acc, bb[k]);
-                n += bc[k];
-                right_area[k] = half_area(acc);
-                right_count[k] = n;
-            }
-            acc = empty_box();
-            n = 0;
-            for (int k = 0; k < BINS - 1; ++k) {
-                acc = join(acc, bb[k]);
-                n += bc[k];
-                if (n == 0 || right_count[k + 1] == 0) continue;
-                const float c = n * half_area(acc) + right_count[k + 1] * right_area[k + 1];
-                if (c < best_cost) { best_cost = c; best_axis = a; best_split = k + 1; }
+                const int b = sah_bin(cen[3 * id + a], clo[a], scale[a]);
+                ++bins.cnt[a][b];
+                for (int c = 0; c < 3; ++c) {
+                    bins.lo[a][b][c] = fminf(bins.lo[a][b][c], prims[id].lo[c]);
+                    bins.hi[a][b][c] = fmaxf(bins.hi[a][b][c], prims[id].hi[c]);
+                }
             }
         }
-        if (best_axis < 0) continue;  // all centroids coincide: keep as a leaf
-        const float ext = chi[best_axis] - clo[best_axis], scale = BINS / ext;
-        auto left_of = [&](int id) {
-            int b = (int)((cen[3 * id + best_axis] - clo[best_axis]) * scale);
-            b = std::min(std::max(b, 0), BINS - 1);
-            return b < best_split;
-        };
+        int axis, split;
+        sah_choose(bins, ext, axis, split);
+        if (axis < 0) continue;  // all centroids coincide: keep as a leaf
+        auto left_of = [&](int id) { return sah_bin(cen[3 * id + axis], clo[axis], scale[axis]) < split; };
         int32_t* beg = out.order.data() + first;
-        int32_t* mid = std::partition(beg, beg + count, left_of);
+        int32_t* mid = std::stable_partition(beg, beg + count, left_of);
         const uint32_t nl = (uint32_t)(mid - beg);
         if (nl == 0 || nl == count) continue;
         const uint32_t L = out.used++, R = out.used++;
         out.left_first[L] = first; out.prim_count[L] = nl;
         out.left_first[R] = first + nl; out.prim_count[R] = count - nl;
         out.left_first[node] = L; out.prim_count[node] = 0;
-        for (uint32_t c : {L, R}) {
-            Box3 b = empty_box();
-            for (uint32_t i = out.left_first[c]; i < out.left_first[c] + out.prim_count[c]; ++i)
-                b = join(b, prims[out.order[i]]);
-            out.box[c] = b;
-            todo.push_back(c);
-        }
+        sah_sides(bins, axis, split, out.box[L], out.box[R]);
+        todo.push_back(L);
+        todo.push_back(R);
     }
 }
 
 void collapse_to_wide(const BinaryBVH& bin, std::vector<Node4>& out, int& depth) {
     out.clear();
     depth = 0;
-    struct Item { uint32_t bin_node; int wide_index; int level; };
+    struct Item { uint32_t bin_node; int level; };
     auto set_child = [&](Node4& n, int c, uint32_t bnode, int32_t ref, int32_t cnt) {
         const Box3& b = bin.box[bnode];
         n.lo_x[c] = b.lo[0]; n.lo_y[c] = b.lo[1]; n.lo_z[c] = b.lo[2];
@@ -207,41 +172,26 @@ void collapse_to_wide(const BinaryBVH& bin, std::vector<Node4>& out, int& depth)
             n.count[c] = 0;
         }
     };
+    // breadth first: wide node w is queue entry w, its inner children are
+    // numbered in order as they are queued
+    std::vector<Item> queue{{0u, 1}};
     out.emplace_back();
     blank(out[0]);
-    std::vector<Item> todo{{0u, 0, 1}};
-    while (!todo.empty()) {
-        Item it = todo.back();
-        todo.pop_back();
+    for (size_t w = 0; w < queue.size(); ++w) {
+        const Item it = queue[w];
         depth = std::max(depth, it.level);
-        // gather up to 4 children by opening the largest inner child repeatedly
-        std::vector<uint32_t> kids;
-        if (bin.prim_count[it.bin_node] > 0) kids.push_back(it.bin_node);  // the root itself is a leaf
-        else { kids.push_back(bin.left_first[it.bin_node]); kids.push_back(bin.left_first[it.bin_node] + 1); }
-        while (kids.size() < 4) {
-            int pick = -1;
-            float best = -1;
-            for (size_t k = 0; k < kids.size(); ++k)
-                if (bin.prim_count[kids[k]] == 0) {
-                    const float a = half_area(bin.box[kids[k]]);
-                    if (a > best) { best = a; pick = (int)k; }
-                }
-            if (pick < 0) break;
-            const uint32_t b = kids[pick];
-            kids.erase(kids.begin() + pick);
-            kids.push_back(bin.left_first[b]);
-            kids.push_back(bin.left_first[b] + 1);
-        }
-        for (size_t c = 0; c < kids.size(); ++c) {
+        uint32_t kids[4];
+        const int n = wide_kids(it.bin_node, bin.box.data(), bin.left_first.data(), bin.prim_count.data(), kids);
+        for (int c = 0; c < n; ++c) {
             const uint32_t b = kids[c];
             if (bin.prim_count[b] > 0) {
-                set_child(out[it.wide_index], (int)c, b, ~(int32_t)bin.left_first[b], (int32_t)bin.prim_count[b]);
+                set_child(out[w], c, b, ~(int32_t)bin.left_first[b], (int32_t)bin.prim_count[b]);
             } else {
                 const int idx = (int)out.size();
                 out.emplace_back();
                 blank(out.back());
-                set_child(out[it.wide_index], (int)c, b, idx, 0);
-                todo.push_back({b, idx, it.level + 1});
+                set_child(out[w], c, b, idx, 0);
+                queue.push_back({b, it.level + 1});
             }
         }
     }

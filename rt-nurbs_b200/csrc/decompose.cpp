@@ -7,82 +7,16 @@
 // float with the reference's order of operations (alpha from knot ratios,
 // then alpha*Q[k] + (1-alpha)*Q[k-1] per coordinate), so on degrees the
 // reference supports the control points are bit-identical to getPatch's.
+// The per-line step (split_axis) lives in scene_math.h, shared with the
+// device builder.
 // Unlike the reference (NURBS_MAX_DEGREE = 4, src/constants.h:31-32) degrees
 // up to NRT_MAX_DEGREE are accepted.
 #include <cmath>
 #include <cstring>
 
-#include "nrt_internal.h"
+#include "scene_math.h"
 
 namespace nrt {
-
-namespace {
-
-struct P4 {
-    float x, y, z, w;
-};
-
-// Breakpoints of a clamped knot vector: U[p], each new interior value, U[last-p].
-// (segs(), src/math/bezier_patch.h:46-53)
-int spans(const float* U, int last, int p, float* out) {
-    int nb = 0;
-    out[nb++] = U[p];
-    for (int i = p + 1; i <= last - p - 1; ++i)
-        if (U[i] != U[i - 1]) out[nb++] = U[i];
-    out[nb] = U[last - p];
-    return nb;
-}
-
-// Strided 2D view: element (k, r) with k along the split direction.
-struct View {
-    P4* base;
-    long sk, sr, piece;  // stride along k, across r, between pieces
-    P4& at(int piece_idx, int k, int r) const { return base[piece_idx * piece + k * sk + r * sr]; }
-};
-
-// Split `lines` curves of degree `deg` (knots K[0..last]) into Bezier pieces.
-int split_axis(const P4* src, long src_sk, long src_sr, int lines, int deg, const float* K, int last, View dst) {
-    float alpha[NRT_MAX_DEGREE + 1];
-    int a = deg, b = deg + 1, nb = 0;
-    for (int k = 0; k <= deg; ++k)
-        for (int r = 0; r < lines; ++r) dst.at(0, k, r) = src[k * src_sk + r * src_sr];
-    while (b < last) {
-        const int first = b;
-        while (b < last && K[b + 1] == K[b]) ++b;
-        const int mult = b - first + 1;
-        if (mult < deg) {
-            const float numer = K[b] - K[a];
-            for (int j = deg; j > mult; --j) alpha[j - mult - 1] = numer / (K[a + j] - K[a]);
-            const int inserts = deg - mult;
-            for (int j = 1; j <= inserts; ++j) {
-                const int s = mult + j;
-                for (int k = deg; k >= s; --k) {
-                    const float al = alpha[k - s], be = 1.0f - al;
-                    for (int r = 0; r < lines; ++r) {
-                        P4& cur = dst.at(nb, k, r);
-                        const P4& prev = dst.at(nb, k - 1, r);
-                        cur.x = al * cur.x + be * prev.x;
-                        cur.y = al * cur.y + be * prev.y;
-                        cur.z = al * cur.z + be * prev.z;
-                        cur.w = al * cur.w + be * prev.w;
-                    }
-                }
-                if (b < last)  // the next piece starts with this one's last points
-                    for (int r = 0; r < lines; ++r) dst.at(nb + 1, inserts - j, r) = dst.at(nb, deg, r);
-            }
-        }
-        ++nb;
-        if (b < last) {
-            for (int k = deg - mult; k <= deg; ++k)
-                for (int r = 0; r < lines; ++r) dst.at(nb, k, r) = src[(b - deg + k) * src_sk + r * src_sr];
-            a = b;
-            ++b;
-        }
-    }
-    return nb;
-}
-
-}  // namespace
 
 int check_surface(const nrt_nurbs_surface& s) {
     if (!s.control_points || !s.u_knots || !s.v_knots)
@@ -112,8 +46,8 @@ int decompose_surface(const nrt_nurbs_surface& s, std::vector<float>& cp, std::v
                       int& nbV) {
     if (int st = check_surface(s)) return st;
     std::vector<float> bu(s.n - s.p + 2), bv(s.m - s.q + 2);
-    nbU = spans(s.u_knots, s.n + s.p + 1, s.p, bu.data());
-    nbV = spans(s.v_knots, s.m + s.q + 1, s.q, bv.data());
+    nbU = knot_spans(s.u_knots, s.n + s.p + 1, s.p, bu.data());
+    nbV = knot_spans(s.v_knots, s.m + s.q + 1, s.q, bv.data());
     const int cols = s.m + 1;
     const long strip = (long)(s.p + 1) * cols, piece = (long)(s.p + 1) * (s.q + 1);
     std::vector<P4> strips((size_t)(nbU + 1) * strip);
@@ -138,18 +72,8 @@ int decompose_surface(const nrt_nurbs_surface& s, std::vector<float>& cp, std::v
 
 void patch_boxes(const PatchSet& ps, std::vector<Box3>& out) {
     out.resize(ps.count());
-    for (int k = 0; k < ps.count(); ++k) {
-        const int n = (ps.deg[2 * k] + 1) * (ps.deg[2 * k + 1] + 1);
-        const float* c = &ps.cp[4 * (size_t)ps.off[k]];
-        Box3 b{{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}};
-        for (int i = 0; i < n; ++i)  // BezierPatchOps::bounds, bezier_patch.h:158-165
-            for (int a = 0; a < 3; ++a) {
-                const float x = c[4 * i + a] / c[4 * i + 3];
-                b.lo[a] = fminf(b.lo[a], x);
-                b.hi[a] = fmaxf(b.hi[a], x);
-            }
-        out[k] = b;
-    }
+    for (int k = 0; k < ps.count(); ++k)
+        out[k] = patch_box(&ps.cp[4 * (size_t)ps.off[k]], (ps.deg[2 * k] + 1) * (ps.deg[2 * k + 1] + 1));
 }
 
 }  // namespace nrt

@@ -13,6 +13,8 @@
 
 #include "kernels.h"
 #include "nrt_internal.h"
+#include "scene_build.h"
+#include "slot_pack.cuh"
 #include "wavefront.h"
 
 // ---------------------------------------------------------------------------
@@ -39,7 +41,7 @@ int fail(int status, const char* fmt, ...) {
     return status;
 }
 
-static int cuda_fail(cudaError_t e, const char* what) {
+int cuda_fail(cudaError_t e, const char* what) {
     return fail(e == cudaErrorMemoryAllocation ? NRT_ERR_NOMEM : NRT_ERR_CUDA, "%s: %s (%s)", what,
                 cudaGetErrorName(e), cudaGetErrorString(e));
 }
@@ -49,199 +51,6 @@ static int cuda_fail(cudaError_t e, const char* what) {
         cudaError_t e_ = (call);                           \
         if (e_ != cudaSuccess) return cuda_fail(e_, what); \
     } while (0)
-
-// Flatness of a patch: largest distance from a control point to the bilinear
-// interpolation of the four corners at its (i/p, j/q) node; patchDelta,
-// src/core/main.cpp:18-43.
-static float patch_delta(const float* P, int p, int q) {
-    const int row = q + 1;
-    auto dh = [&](int i, float o[3]) {
-        const float iw = 1.0f / P[4 * i + 3];
-        o[0] = P[4 * i] * iw; o[1] = P[4 * i + 1] * iw; o[2] = P[4 * i + 2] * iw;
-    };
-    float c00[3], c10[3], c01[3], c11[3];
-    dh(0, c00); dh(p * row, c10); dh(q, c01); dh(p * row + q, c11);
-    float d = 0.f;
-    for (int i = 0; i <= p; ++i)
-        for (int j = 0; j <= q; ++j) {
-            const float u = (float)i / p, v = (float)j / q;
-            const float a = (1 - u) * (1 - v), b = u * (1 - v), c = (1 - u) * v, e = u * v;
-            float Pij[3];
-            dh(i * row + j, Pij);
-            float s = 0.f;
-            for (int k = 0; k < 3; ++k) {
-                const float B = a * c00[k] + b * c10[k] + c * c01[k] + e * c11[k];
-                s += (Pij[k] - B) * (Pij[k] - B);
-            }
-            d = fmaxf(d, sqrtf(s));
-        }
-    return d;
-}
-
-// Oriented bounding box of a patch's dehomogenised control points (their
-// convex hull holds the patch when every weight is positive): axes from the
-// principal directions of the points (cyclic Jacobi on the 3x3 covariance, in
-// double), extents from the points' projections.  Four float4 per slot:
-// (axis_k, half extent_k) for k = 0..2, then (centre, 0).  A patch with a
-// non-positive weight gets infinite extents, so that it is never culled.
-static void patch_obb(const float* P, int p, int q, float4 out[4]) {
-    const int n = (p + 1) * (q + 1);
-    std::vector<double> X(3 * (size_t)n);
-    bool pos = true;
-    double m[3] = {0, 0, 0};
-    for (int i = 0; i < n; ++i) {
-        const double w = P[4 * i + 3];
-        pos = pos && w > 0.0;
-        for (int k = 0; k < 3; ++k) {
-            X[3 * i + k] = w != 0.0 ? P[4 * i + k] / w : 0.0;
-            m[k] += X[3 * i + k] / n;
-        }
-    }
-    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-    for (int i = 0; i < n; ++i)
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) A[a][b] += (X[3 * i + a] - m[a]) * (X[3 * i + b] - m[b]);
-    for (int sweep = 0; sweep < 32; ++sweep) {
-        const double off = std::fabs(A[0][1]) + std::fabs(A[0][2]) + std::fabs(A[1][2]);
-        if (off <= 1e-300 + 1e-15 * (std::fabs(A[0][0]) + std::fabs(A[1][1]) + std::fabs(A[2][2]))) break;
-        for (int a = 0; a < 2; ++a)
-            for (int b = a + 1; b < 3; ++b) {
-                if (A[a][b] == 0.0) continue;
-                const double th = 0.5 * std::atan2(2.0 * A[a][b], A[b][b] - A[a][a]);
-                const double c = std::cos(th), s = std::sin(th);
-                for (int k = 0; k < 3; ++k) {  // A <- A J
-                    const double ka = A[k][a], kb = A[k][b];
-                    A[k][a] = c * ka - s * kb;
-                    A[k][b] = s * ka + c * kb;
-                }
-                for (int k = 0; k < 3; ++k) {  // A <- J^T A
-                    const double ak = A[a][k], bk = A[b][k];
-                    A[a][k] = c * ak - s * bk;
-                    A[b][k] = s * ak + c * bk;
-                }
-                for (int k = 0; k < 3; ++k) {  // V <- V J
-                    const double ka = V[k][a], kb = V[k][b];
-                    V[k][a] = c * ka - s * kb;
-                    V[k][b] = s * ka + c * kb;
-                }
-            }
-    }
-    double ctr[3] = {m[0], m[1], m[2]}, half[3];
-    for (int a = 0; a < 3; ++a) {
-        // round the axis to float first: the device projects with the stored axis
-        float ax[3] = {(float)V[0][a], (float)V[1][a], (float)V[2][a]};
-        double lo = 1e300, hi = -1e300;
-        for (int i = 0; i < n; ++i) {
-            const double t = ax[0] * (X[3 * i] - m[0]) + ax[1] * (X[3 * i + 1] - m[1]) + ax[2] * (X[3 * i + 2] - m[2]);
-            lo = std::min(lo, t);
-            hi = std::max(hi, t);
-        }
-        half[a] = 0.5 * (hi - lo);
-        for (int k = 0; k < 3; ++k) ctr[k] += ax[k] * 0.5 * (lo + hi);
-        out[a] = make_float4(ax[0], ax[1], ax[2], 0.f);
-    }
-    double cmax = 0.0;
-    for (int k = 0; k < 3; ++k) cmax = std::max(cmax, std::fabs(ctr[k]));
-    for (int a = 0; a < 3; ++a) {
-        // extents cover the float-rounded centre and axes
-        const double h = half[a] * (1.0 + 1e-6) + 4e-7 * cmax + 1e-30;
-        out[a].w = pos ? (float)(h * (1.0 + 1e-6)) : INFINITY;
-    }
-    out[3] = make_float4((float)ctr[0], (float)ctr[1], (float)ctr[2], 0.f);
-}
-
-// Frame of the learned guess's features (see mlp.cuh): the tangent frame of
-// the patch at (u, v) = (1/2, 1/2), in patch-local coordinates.  Axes A = dS/du,
-// B = dS/dv and the normal of A x B scaled by sqrt|A x B|; origin
-// S(1/2, 1/2) - A/2 - B/2, so that a point's frame coordinates (s, t) are its
-// (u, v) to first order (the iterate of one Newton step from the midpoint).
-// Rational evaluation in double from the weighted-homogeneous points.
-// Degenerate nets (collapsed tangents) fall back to the box, normalised.
-static dev::PatchFrame patch_frame(const float* P, int p, int q, double cx, double cy, double cz, const Box3& b,
-                                   float delta) {
-    auto pt = [&](int i, int j, double o[3]) {
-        const float* c = P + 4 * (i * (q + 1) + j);
-        o[0] = c[0] / (double)c[3] - cx; o[1] = c[1] / (double)c[3] - cy; o[2] = c[2] / (double)c[3] - cz;
-    };
-    // Bernstein values and derivatives at 1/2
-    auto bern = [](int n, double* B, double* dB) {
-        double c = 1.0;
-        for (int i = 0; i <= n; ++i) {
-            B[i] = c / std::ldexp(1.0, n);
-            c = c * (n - i) / (i + 1);
-        }
-        double cm = 1.0, Bm[8];
-        for (int i = 0; i < n; ++i) {
-            Bm[i] = cm / std::ldexp(1.0, n - 1);
-            cm = cm * (n - 1 - i) / (i + 1);
-        }
-        for (int i = 0; i <= n; ++i) dB[i] = n * ((i > 0 ? Bm[i - 1] : 0.0) - (i < n ? Bm[i] : 0.0));
-    };
-    double Bu[8], dBu[8], Bv[8], dBv[8];
-    bern(p, Bu, dBu);
-    bern(q, Bv, dBv);
-    double H[4] = {0, 0, 0, 0}, Hu[4] = {0, 0, 0, 0}, Hv[4] = {0, 0, 0, 0};
-    for (int i = 0; i <= p; ++i)
-        for (int j = 0; j <= q; ++j) {
-            const float* c = P + 4 * (i * (q + 1) + j);
-            const double w = c[3];
-            const double X[4] = {c[0] - w * cx, c[1] - w * cy, c[2] - w * cz, w};
-            for (int k = 0; k < 4; ++k) {
-                H[k] += Bu[i] * Bv[j] * X[k];
-                Hu[k] += dBu[i] * Bv[j] * X[k];
-                Hv[k] += Bu[i] * dBv[j] * X[k];
-            }
-        }
-    double A[3], B[3], o[3];
-    for (int k = 0; k < 3; ++k) {
-        const double S = H[k] / H[3];
-        A[k] = (Hu[k] - S * Hu[3]) / H[3];
-        B[k] = (Hv[k] - S * Hv[3]) / H[3];
-        o[k] = S - 0.5 * A[k] - 0.5 * B[k];
-    }
-    const double N[3] = {A[1] * B[2] - A[2] * B[1], A[2] * B[0] - A[0] * B[2], A[0] * B[1] - A[1] * B[0]};
-    const double nn = std::sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
-    const double aa = A[0] * A[0] + A[1] * A[1] + A[2] * A[2], bb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
-    dev::PatchFrame f{};
-    double M[3][3];  // columns A, B, N/sqrt|N|
-    double scale;
-    if (nn > 1e-9 * (aa + bb) && aa > 0 && bb > 0) {
-        const double s = 1.0 / std::sqrt(nn);
-        for (int k = 0; k < 3; ++k) { M[k][0] = A[k]; M[k][1] = B[k]; M[k][2] = N[k] * s; }
-        scale = std::sqrt(std::max(aa, bb));
-    } else {
-        for (int k = 0; k < 3; ++k) {
-            o[k] = (double)b.lo[k] - (k == 0 ? cx : k == 1 ? cy : cz);
-            for (int l = 0; l < 3; ++l) M[k][l] = k == l ? std::max((double)b.hi[k] - b.lo[k], 1e-12) : 0.0;
-        }
-        scale = std::max({M[0][0], M[1][1], M[2][2]});
-    }
-    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
-                       M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
-                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
-    const double id = 1.0 / det;
-    const double inv[9] = {(M[1][1] * M[2][2] - M[1][2] * M[2][1]) * id, (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id,
-                           (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id, (M[1][2] * M[2][0] - M[1][0] * M[2][2]) * id,
-                           (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id, (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id,
-                           (M[1][0] * M[2][1] - M[1][1] * M[2][0]) * id, (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id,
-                           (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id};
-    f.ox = (float)o[0]; f.oy = (float)o[1]; f.oz = (float)o[2];
-    for (int k = 0; k < 9; ++k) f.m[k] = (float)inv[k];
-    double hmax = 0.0;  // half-thickness of the control net along the frame's h axis
-    for (int i = 0; i <= p; ++i)
-        for (int j = 0; j <= q; ++j) {
-            double X[3];
-            pt(i, j, X);
-            const double d3[3] = {X[0] - o[0], X[1] - o[1], X[2] - o[2]};
-            hmax = std::max(hmax, std::fabs(inv[6] * d3[0] + inv[7] * d3[1] + inv[8] * d3[2]));
-        }
-    f.slab = (float)std::max(hmax, 1e-6);
-    f.flat = (float)(hmax * std::sqrt(std::fabs(det)) / std::max(scale * scale, 1e-30));
-    (void)delta;
-    f.lo[0] = (float)(b.lo[0] - cx); f.lo[1] = (float)(b.lo[1] - cy); f.lo[2] = (float)(b.lo[2] - cz);
-    f.hi_x = (float)(b.hi[0] - cx); f.hi_y = (float)(b.hi[1] - cy); f.hi_z = (float)(b.hi[2] - cz);
-    return f;
-}
 
 dev::MlpParams blob_params(const void* blob);
 size_t mlp_blob_bytes();
@@ -256,7 +65,6 @@ struct nrt_scene {
     int device = 0;
     PatchSet ps;
     int n_surfaces = 0;
-    std::vector<int32_t> slot_patch;   // device slot -> global patch id
     void* arena = nullptr;
     size_t arena_bytes = 0;
     unsigned long long* counters = nullptr;
@@ -290,9 +98,98 @@ struct nrt_scene {
     long long newton_launches = 0;
 };
 
+namespace nrt {
 
+// The scene's device arena: one allocation, every array 256-byte aligned, in
+// this order.  Both builders lay it out the same way.
+ArenaLayout arena_layout(size_t n_wide, int N, size_t n_floats) {
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    ArenaLayout L{};
+    size_t at = 0;
+    auto take = [&](size_t bytes) { const size_t r = at; at += align(bytes); return r; };
+    L.nodes = take(n_wide * sizeof(Node4));
+    L.hdr = take(N * sizeof(int4));
+    L.centre = take(N * sizeof(double4));
+    L.cp = take(n_floats * sizeof(float));
+    L.corners = take(4 * (size_t)N * sizeof(float4));
+    L.delta = take(N * sizeof(float));
+    L.counters = take(dev::kCounterWords * sizeof(unsigned long long));
+    L.rank = take(N * sizeof(int32_t));
+    L.frames = take(N * sizeof(dev::PatchFrame));
+    L.obb = take(4 * (size_t)N * sizeof(float4));
+    L.leafbox = take(2 * (size_t)N * sizeof(float4));
+    L.total = at;
+    return L;
+}
 
-namespace {
+// The wavefront's degree classes from the per-(p, q) patch counts: one class
+// per degree pair present, in increasing p | q << 4, ranks assigned in that
+// order (slots keep their order inside a class).
+void plan_classes(const int* degree_hist, int N, dev::WfPlan& plan) {
+    plan = dev::WfPlan{};
+    plan.n_slots = N;
+    int rank = 0;
+    for (int key = 0; key < 256; ++key) {
+        const int p = key & 15, q = key >> 4;
+        if (p < 1 || q < 1 || p > NRT_MAX_DEGREE || q > NRT_MAX_DEGREE) continue;
+        const int cnt = degree_hist[p * 8 + q];
+        if (cnt == 0) continue;
+        plan.class_pq[plan.n_classes] = key;
+        plan.class_rank[plan.n_classes] = rank;
+        plan.class_grid[plan.n_classes] = 148 * 4;
+        ++plan.n_classes;
+        rank += cnt;
+    }
+    plan.class_rank[plan.n_classes] = N;
+}
+
+// A scene object with its arena allocated (zero-filled) on the build's device.
+int new_scene(const nrt_build_opts& o, const ArenaLayout& L, nrt_scene** out, char** arena) {
+    nrt_scene* sc = new (std::nothrow) nrt_scene();
+    if (!sc) return fail(NRT_ERR_NOMEM, "host allocation failed");
+    sc->device = o.device;
+    sc->wf_chunk = o.wavefront_chunk > 0 ? o.wavefront_chunk : (1LL << 23);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaError_t e = cudaSetDevice(o.device);
+    if (e != cudaSuccess) { delete sc; return cuda_fail(e, "cudaSetDevice"); }
+    e = cudaMalloc(&sc->arena, L.total);
+    if (e == cudaSuccess) e = cudaMemset(sc->arena, 0, L.total);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        if (sc->arena) cudaFree(sc->arena);
+        delete sc;
+        return cuda_fail(e, "cudaMalloc(scene)");
+    }
+    sc->arena_bytes = L.total;
+    *out = sc;
+    *arena = static_cast<char*>(sc->arena);
+    return NRT_OK;
+}
+
+// Points the scene's views at its filled arena and records the rest.
+void finish_scene(nrt_scene* sc, const ArenaLayout& L, int N, dev::WfPlan plan, nrt_scene_info info, PatchSet&& ps,
+                  int n_surfaces) {
+    char* base = static_cast<char*>(sc->arena);
+    sc->view.nodes = reinterpret_cast<const dev::Node4*>(base + L.nodes);
+    sc->view.hdr = reinterpret_cast<const int4*>(base + L.hdr);
+    sc->view.centre = reinterpret_cast<const double4*>(base + L.centre);
+    sc->view.cp = reinterpret_cast<const float*>(base + L.cp);
+    sc->view.corners = reinterpret_cast<const float4*>(base + L.corners);
+    sc->view.delta = reinterpret_cast<const float*>(base + L.delta);
+    sc->counters = reinterpret_cast<unsigned long long*>(base + L.counters);
+    plan.rank_of = reinterpret_cast<const int32_t*>(base + L.rank);
+    sc->view.frames = reinterpret_cast<const dev::PatchFrame*>(base + L.frames);
+    sc->view.obb = reinterpret_cast<const float4*>(base + L.obb);
+    sc->view.leafbox = reinterpret_cast<const float4*>(base + L.leafbox);
+    sc->view.n_slots = N;
+    sc->plan = plan;
+    info.n_patches = N;
+    info.device_bytes = L.total;
+    sc->info = info;
+    sc->ps = std::move(ps);
+    sc->n_surfaces = n_surfaces;
+}
 
 int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_scene** out) {
     if (!out) return fail(NRT_ERR_INVALID, "out is null");
@@ -303,6 +200,8 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
     if (opts) o = *opts;
     if (o.wavefront_chunk < 0) return fail(NRT_ERR_INVALID, "negative wavefront_chunk");
     if (o.max_leaf < 1 || o.max_leaf > 8) return fail(NRT_ERR_INVALID, "max_leaf must be in 1..8");
+    if (o.builder != NRT_BVH_BINNED_SAH && o.builder != NRT_BVH_EXACT_SAH)
+        return fail(NRT_ERR_INVALID, "unknown BVH builder %d", o.builder);
     if (N >= (1 << 27)) return fail(NRT_ERR_INVALID, "too many patches (%d)", N);
     for (int k = 0; k < N; ++k) {
         const int p = ps.deg[2 * k], q = ps.deg[2 * k + 1];
@@ -339,133 +238,67 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
                     leafbox[2 * (size_t)k + 1] = make_float4(nd.hi_x[c], nd.hi_y[c], nd.hi_z[c], 0.f);
                 }
     std::vector<float> blocks;
-    std::vector<int32_t> slot_patch(N);
     size_t total_floats = 0;
     for (int s = 0; s < N; ++s) {
         const int k = bin.order[s];
         total_floats += 4 * (size_t)dev::padded_points(ps.deg[2 * k], ps.deg[2 * k + 1]);
     }
+    if (total_floats >= ((size_t)1 << 31))
+        return fail(NRT_ERR_INVALID, "scene too large (%zu block floats)", total_floats);
     blocks.assign(total_floats, 0.f);
     size_t off = 0;
     nrt_scene_info info{};
     for (int s = 0; s < N; ++s) {
         const int k = bin.order[s];
-        slot_patch[s] = k;
-        const int p = ps.deg[2 * k], q = ps.deg[2 * k + 1], n = (p + 1) * (q + 1);
-        const int np = dev::padded_points(p, q);
-        const float* P = &ps.cp[4 * (size_t)ps.off[k]];
-        const Box3& b = boxes[k];
-        const double cx = 0.5 * ((double)b.lo[0] + b.hi[0]), cy = 0.5 * ((double)b.lo[1] + b.hi[1]),
-                     cz = 0.5 * ((double)b.lo[2] + b.hi[2]);
-        bool pos = true;
-        double rad = 0.0;
-        for (int i = 0; i < n; ++i) {
-            const double w = P[4 * i + 3];
-            pos = pos && (w > 0.0);
-            blocks[off + i] = (float)((double)P[4 * i + 0] - w * cx);
-            blocks[off + np + i] = (float)((double)P[4 * i + 1] - w * cy);
-            blocks[off + 2 * np + i] = (float)((double)P[4 * i + 2] - w * cz);
-            blocks[off + 3 * np + i] = (float)w;
-            if (w != 0.0) {
-                const double dx = P[4 * i] / w - cx, dy = P[4 * i + 1] / w - cy, dz = P[4 * i + 2] / w - cz;
-                rad = std::max(rad, std::sqrt(dx * dx + dy * dy + dz * dz));
-            }
-        }
-        for (int i = n; i < np; ++i) blocks[off + 3 * np + i] = 1.f;  // padding never read as a point
-        hdr[s] = make_int4((int)off, p | (q << 4) | ((pos ? dev::kFlagPositiveWeights : 0) << 8), k, ps.surf[k]);
-        centre[s] = make_double4(cx, cy, cz, rad);
-        const int ci[4] = {0, p * (q + 1), p * (q + 1) + q, q};  // q00, q10, q11, q01 (bezier_patch.h:37-44)
-        for (int c = 0; c < 4; ++c) {
-            const float* X = P + 4 * ci[c];
-            const float iw = 1.f / X[3];
-            corners[4 * (size_t)s + c] = make_float4(X[0] * iw, X[1] * iw, X[2] * iw, 0.f);
-        }
-        delta[s] = patch_delta(P, p, q);
-        frames[s] = patch_frame(P, p, q, cx, cy, cz, b, delta[s]);
-        patch_obb(P, p, q, &obbs[4 * (size_t)s]);
+        const int p = ps.deg[2 * k], q = ps.deg[2 * k + 1];
+        pack_slot(&ps.cp[4 * (size_t)ps.off[k]], p, q, boxes[k], k, ps.surf[k], (long long)off, &blocks[off], hdr[s],
+                  centre[s], &corners[4 * (size_t)s], delta[s], frames[s], &obbs[4 * (size_t)s]);
         info.degree_hist[p * 8 + q] += 1;
-        off += 4 * (size_t)np;
+        off += 4 * (size_t)dev::padded_points(p, q);
     }
 
-    // One device arena, every array 256-byte aligned.
-    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t sz_nodes = align(wide.size() * sizeof(Node4)), sz_hdr = align(N * sizeof(int4)),
-                 sz_cen = align(N * sizeof(double4)), sz_cp = align(blocks.size() * sizeof(float)),
-                 sz_cor = align(corners.size() * sizeof(float4)), sz_del = align(N * sizeof(float)),
-                 sz_ctr = align(dev::kCounterWords * sizeof(unsigned long long)),
-                 sz_rank = align(N * sizeof(int32_t)), sz_frm = align(N * sizeof(dev::PatchFrame)),
-                 sz_obb = align(obbs.size() * sizeof(float4)), sz_lbx = align(leafbox.size() * sizeof(float4));
-    const size_t total =
-        sz_nodes + sz_hdr + sz_cen + sz_cp + sz_cor + sz_del + sz_ctr + sz_rank + sz_frm + sz_obb + sz_lbx;
-    // wavefront plan: patches ranked by (p, q, slot); one class per degree pair present
-    std::vector<int32_t> by_rank(N), rank_of(N);
-    for (int s2 = 0; s2 < N; ++s2) by_rank[s2] = s2;
-    std::stable_sort(by_rank.begin(), by_rank.end(), [&](int a, int b) { return (hdr[a].y & 0xff) < (hdr[b].y & 0xff); });
+    // wavefront plan: patches ranked by (p, q, slot)
     dev::WfPlan plan{};
-    plan.n_slots = N;
-    for (int rk = 0; rk < N; ++rk) {
-        rank_of[by_rank[rk]] = rk;
-        const int pq = hdr[by_rank[rk]].y & 0xff;
-        if (plan.n_classes == 0 || plan.class_pq[plan.n_classes - 1] != pq) {
-            plan.class_pq[plan.n_classes] = pq;
-            plan.class_rank[plan.n_classes] = rk;
-            plan.class_grid[plan.n_classes] = 148 * 4;
-            ++plan.n_classes;
-        }
+    plan_classes(info.degree_hist, N, plan);
+    std::vector<int32_t> rank_of(N);
+    {
+        int next[256] = {0};
+        for (int c = 0; c < plan.n_classes; ++c) next[plan.class_pq[c]] = plan.class_rank[c];
+        for (int s2 = 0; s2 < N; ++s2) rank_of[s2] = next[hdr[s2].y & 0xff]++;
     }
-    plan.class_rank[plan.n_classes] = N;
-    nrt_scene* sc = new (std::nothrow) nrt_scene();
-    if (!sc) return fail(NRT_ERR_NOMEM, "host allocation failed");
-    sc->device = o.device;
-    sc->wf_chunk = o.wavefront_chunk > 0 ? o.wavefront_chunk : (1LL << 23);
-    int prev = 0;
-    cudaGetDevice(&prev);
-    cudaError_t e = cudaSetDevice(o.device);
-    if (e != cudaSuccess) { delete sc; return cuda_fail(e, "cudaSetDevice"); }
-    e = cudaMalloc(&sc->arena, total);
-    if (e != cudaSuccess) { delete sc; cudaSetDevice(prev); return cuda_fail(e, "cudaMalloc(scene)"); }
-    char* base = static_cast<char*>(sc->arena);
-    size_t at = 0;
-    auto put = [&](const void* src, size_t bytes, size_t slot) -> void* {
-        void* dst = base + at;
-        if (bytes) e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
-        at += slot;
-        return dst;
+    const ArenaLayout L = arena_layout(wide.size(), N, blocks.size());
+    nrt_scene* sc = nullptr;
+    char* base = nullptr;
+    if (int st = new_scene(o, L, &sc, &base)) return st;
+    cudaError_t e = cudaSuccess;
+    auto put = [&](size_t at, const void* src, size_t bytes) {
+        if (bytes && e == cudaSuccess) e = cudaMemcpy(base + at, src, bytes, cudaMemcpyHostToDevice);
     };
-    sc->view.nodes = static_cast<const dev::Node4*>(put(wide.data(), wide.size() * sizeof(Node4), sz_nodes));
-    sc->view.hdr = static_cast<const int4*>(put(hdr.data(), N * sizeof(int4), sz_hdr));
-    sc->view.centre = static_cast<const double4*>(put(centre.data(), N * sizeof(double4), sz_cen));
-    sc->view.cp = static_cast<const float*>(put(blocks.data(), blocks.size() * sizeof(float), sz_cp));
-    sc->view.corners = static_cast<const float4*>(put(corners.data(), corners.size() * sizeof(float4), sz_cor));
-    sc->view.delta = static_cast<const float*>(put(delta.data(), N * sizeof(float), sz_del));
-    sc->counters = reinterpret_cast<unsigned long long*>(base + at);
-    if (e == cudaSuccess) e = cudaMemset(sc->counters, 0, sz_ctr);
-    at += sz_ctr;
-    plan.rank_of = static_cast<const int32_t*>(put(rank_of.data(), N * sizeof(int32_t), sz_rank));
-    sc->view.frames = static_cast<const dev::PatchFrame*>(put(frames.data(), N * sizeof(dev::PatchFrame), sz_frm));
-    sc->view.obb = static_cast<const float4*>(put(obbs.data(), obbs.size() * sizeof(float4), sz_obb));
-    sc->view.leafbox = static_cast<const float4*>(put(leafbox.data(), leafbox.size() * sizeof(float4), sz_lbx));
-    sc->plan = plan;
-    cudaSetDevice(prev);
+    put(L.nodes, wide.data(), wide.size() * sizeof(Node4));
+    put(L.hdr, hdr.data(), N * sizeof(int4));
+    put(L.centre, centre.data(), N * sizeof(double4));
+    put(L.cp, blocks.data(), blocks.size() * sizeof(float));
+    put(L.corners, corners.data(), corners.size() * sizeof(float4));
+    put(L.delta, delta.data(), N * sizeof(float));
+    put(L.rank, rank_of.data(), N * sizeof(int32_t));
+    put(L.frames, frames.data(), N * sizeof(dev::PatchFrame));
+    put(L.obb, obbs.data(), obbs.size() * sizeof(float4));
+    put(L.leafbox, leafbox.data(), leafbox.size() * sizeof(float4));
     if (e != cudaSuccess) {
-        cudaFree(sc->arena);
-        delete sc;
+        nrt_scene_destroy(sc);
         return cuda_fail(e, "scene upload");
     }
-    sc->view.n_slots = N;
-    sc->arena_bytes = total;
-    info.n_patches = N;
     info.n_surfaces = n_surfaces;
     info.n_nodes = (int)wide.size();
     info.bvh_depth = depth;
-    info.device_bytes = total;
-    sc->info = info;
-    sc->slot_patch = std::move(slot_patch);
-    sc->ps = std::move(ps);
-    sc->n_surfaces = n_surfaces;
+    finish_scene(sc, L, N, plan, info, std::move(ps), n_surfaces);
     *out = sc;
     return NRT_OK;
 }
+
+}  // namespace nrt
+
+namespace {
 
 void to_dev_opts(const nrt_intersect_opts& o, dev::Opts& d, int counters) {
     d.nw.max_iter = o.max_iter;
@@ -564,6 +397,7 @@ int nrt_build_bvh_binary(const float* boxes, int n, int builder, float* node_bou
 int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nrt_build_opts* opts,
                      nrt_scene** out) {
     if (!surfaces || n_surfaces <= 0 || !out) return fail(NRT_ERR_INVALID, "null or empty surface list");
+    if (opts && opts->builder == NRT_BVH_BINNED_SAH_DEVICE) return build_scene_device_surfaces(surfaces, n_surfaces, *opts, out);
     PatchSet ps;
     for (int si = 0; si < n_surfaces; ++si) {
         std::vector<float> cp, ranges;
@@ -589,6 +423,8 @@ int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nr
 int nrt_scene_create_from_patches(const float* cp, const int32_t* cp_offset, const int32_t* degrees, int n_patches,
                                   const nrt_build_opts* opts, nrt_scene** out) {
     if (!cp || !cp_offset || !degrees || n_patches <= 0 || !out) return fail(NRT_ERR_INVALID, "null or empty input");
+    if (opts && opts->builder == NRT_BVH_BINNED_SAH_DEVICE)
+        return build_scene_device_patches(cp, cp_offset, degrees, n_patches, *opts, out);
     PatchSet ps;
     int max_point = 0;
     for (int k = 0; k < n_patches; ++k) {
@@ -634,9 +470,22 @@ int nrt_scene_get_info(const nrt_scene* scene, nrt_scene_info* info) {
 
 int nrt_scene_patch_table(const nrt_scene* scene, int32_t* surface_of, float* ranges) {
     if (!scene) return fail(NRT_ERR_INVALID, "null scene");
-    const int N = scene->ps.count();
+    const int N = (int)scene->ps.surf.size();
     if (surface_of) std::memcpy(surface_of, scene->ps.surf.data(), sizeof(int32_t) * N);
     if (ranges) std::memcpy(ranges, scene->ps.ranges.data(), sizeof(float) * 4 * N);
+    return NRT_OK;
+}
+
+int nrt_scene_copy_arena(const nrt_scene* scene, void* host_dst, size_t bytes) {
+    if (!scene || !host_dst) return fail(NRT_ERR_INVALID, "null argument");
+    if (bytes < scene->arena_bytes) return fail(NRT_ERR_INVALID, "buffer of %zu bytes, arena has %zu", bytes,
+                                                scene->arena_bytes);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    const cudaError_t e = cudaMemcpy(host_dst, scene->arena, scene->arena_bytes, cudaMemcpyDeviceToHost);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "nrt_scene_copy_arena");
     return NRT_OK;
 }
 

@@ -34,4 +34,5 @@ from .lib import (  # noqa: F401
     SCHED_WAVEFRONT,
     BVH_BINNED_SAH,
     BVH_EXACT_SAH,
+    BVH_BINNED_SAH_DEVICE,
 )

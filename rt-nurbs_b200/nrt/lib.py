@@ -11,7 +11,7 @@ _LIB = None
 
 INIT_MIDPOINT, INIT_BILINEAR, INIT_LEARNED = 0, 1, 2
 SCHED_PIXEL, SCHED_WAVEFRONT = 0, 1
-BVH_BINNED_SAH, BVH_EXACT_SAH = 0, 1
+BVH_BINNED_SAH, BVH_EXACT_SAH, BVH_BINNED_SAH_DEVICE = 0, 1, 2
 
 
 class NrtError(RuntimeError):
@@ -125,6 +125,7 @@ def lib():
         L.nrt_scene_destroy.argtypes = [vp]
         L.nrt_scene_get_info.argtypes = [vp, C.POINTER(SceneInfo)]
         L.nrt_scene_patch_table.argtypes = [vp, vp, vp]
+        L.nrt_scene_copy_arena.argtypes = [vp, vp, C.c_size_t]
         L.nrt_default_opts.argtypes = [C.POINTER(IntersectOpts)]
         L.nrt_default_opts.restype = None
         L.nrt_reference_opts.argtypes = [C.POINTER(IntersectOpts)]
@@ -304,6 +305,12 @@ class Scene:
         hist = {(k // 8, k % 8): int(v) for k, v in enumerate(inf.degree_hist) if v}
         return {"n_patches": inf.n_patches, "n_surfaces": inf.n_surfaces, "n_nodes": inf.n_nodes,
                 "bvh_depth": inf.bvh_depth, "device_bytes": int(inf.device_bytes), "degree_hist": hist}
+
+    def arena(self) -> np.ndarray:
+        """The scene's device arena as host bytes (nrt_scene_copy_arena)."""
+        out = np.zeros(self.info()["device_bytes"], np.uint8)
+        _check(lib().nrt_scene_copy_arena(self._h, out.ctypes.data, out.nbytes))
+        return out
 
     def patch_table(self):
         n = self.info()["n_patches"]
