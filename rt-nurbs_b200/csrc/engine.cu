@@ -470,9 +470,26 @@ int nrt_scene_get_info(const nrt_scene* scene, nrt_scene_info* info) {
 
 int nrt_scene_patch_table(const nrt_scene* scene, int32_t* surface_of, float* ranges) {
     if (!scene) return fail(NRT_ERR_INVALID, "null scene");
-    const int N = (int)scene->ps.surf.size();
-    if (surface_of) std::memcpy(surface_of, scene->ps.surf.data(), sizeof(int32_t) * N);
-    if (ranges) std::memcpy(ranges, scene->ps.ranges.data(), sizeof(float) * 4 * N);
+    const PatchSet& ps = scene->ps;
+    if (ps.spans.empty()) {
+        const int N = (int)ps.surf.size();
+        if (surface_of) std::memcpy(surface_of, ps.surf.data(), sizeof(int32_t) * N);
+        if (ranges) std::memcpy(ranges, ps.ranges.data(), sizeof(float) * 4 * N);
+        return NRT_OK;
+    }
+    for (size_t si = 0; si < ps.spans.size(); ++si) {  // expanded from the per-surface breakpoints
+        const PatchSet::Spans& sp = ps.spans[si];
+        const float *bu = &ps.breaks[sp.bu], *bv = &ps.breaks[sp.bv];
+        for (int i = 0; i < sp.nbU; ++i)
+            for (int j = 0; j < sp.nbV; ++j) {
+                const size_t k = (size_t)sp.patch0 + (size_t)i * sp.nbV + j;
+                if (surface_of) surface_of[k] = (int32_t)si;
+                if (ranges) {
+                    ranges[4 * k] = bu[i]; ranges[4 * k + 1] = bu[i + 1];
+                    ranges[4 * k + 2] = bv[j]; ranges[4 * k + 3] = bv[j + 1];
+                }
+            }
+    }
     return NRT_OK;
 }
 

@@ -21,6 +21,14 @@ struct PatchSet {
     std::vector<int32_t> deg;     // (p, q) per patch
     std::vector<float> ranges;    // (u0, u1, v0, v1) per patch
     std::vector<int32_t> surf;    // surface index per patch
+    // Instead of ranges/surf (device builder): per surface its first patch,
+    // span counts and the offsets of its u and v breakpoints in `breaks`.
+    struct Spans {
+        int patch0, nbU, nbV;
+        size_t bu, bv;
+    };
+    std::vector<Spans> spans;
+    std::vector<float> breaks;
     int count() const { return (int)off.size(); }
 };
 

@@ -23,7 +23,11 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <memory>
+#include <new>
+#include <thread>
 #include <vector>
 
 #include "scene_build.h"
@@ -34,7 +38,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kBigNode = 4096;   // nodes with more patches get a block, the rest a warp
-constexpr int kBigThreads = 512;
 constexpr int kSmallWarps = 8;
 
 struct SurfDesc {
@@ -183,13 +186,89 @@ __device__ __forceinline__ void bins_add(BinStore& B, const Box3& box, const flo
     }
 }
 
-__device__ __forceinline__ void bins_decode(BinStore& B, int t, int nt) {
-    for (int e = t; e < 3 * kSahBins; e += nt) {
-        const int a = e / kSahBins, k = e % kSahBins;
+// One bin per lane: lane k holds bin k of an axis.
+struct LaneBin {
+    float lo[3], hi[3];
+    int cnt;
+};
+
+__device__ __forceinline__ LaneBin lane_bin(const BinStore& B, int a, int k) {
+    LaneBin b;
+    for (int c = 0; c < 3; ++c) {
+        b.lo[c] = o2f(B.i.lo[a][k][c]);
+        b.hi[c] = o2f(B.i.hi[a][k][c]);
+    }
+    b.cnt = B.i.cnt[a][k];
+    return b;
+}
+
+// sah_choose with a warp: prefix and suffix joins of the bins by shuffles
+// (joins are min / max, so every partial box equals the sequential sweep's),
+// each lane costs the split after its bin, and the cheapest split wins, the
+// earliest (axis, bin) on ties: the sweep's choice.  All lanes return it,
+// with the patch count left of the split.
+__device__ __forceinline__ void warp_choose(const LaneBin (&b)[3], const float ext[3], int lane, int& axis,
+                                            int& split, int& nl) {
+    float best_c = INFINITY;
+    int best_key = 0x7fffffff, best_nl = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (!(ext[a] > 0)) continue;
+        float L[6], R[6];
+        int nL = b[a].cnt, nR = b[a].cnt;
         for (int c = 0; c < 3; ++c) {
-            B.f.lo[a][k][c] = o2f(B.i.lo[a][k][c]);
-            B.f.hi[a][k][c] = o2f(B.i.hi[a][k][c]);
+            L[c] = R[c] = b[a].lo[c];
+            L[3 + c] = R[3 + c] = b[a].hi[c];
         }
+        for (int d = 1; d < 32; d <<= 1) {
+            float t[6];
+            for (int c = 0; c < 6; ++c) t[c] = __shfl_up_sync(kFull, L[c], d);
+            const int tn = __shfl_up_sync(kFull, nL, d);
+            if (lane >= d) {
+                for (int c = 0; c < 3; ++c) { L[c] = fminf(L[c], t[c]); L[3 + c] = fmaxf(L[3 + c], t[3 + c]); }
+                nL += tn;
+            }
+            for (int c = 0; c < 6; ++c) t[c] = __shfl_down_sync(kFull, R[c], d);
+            const int rn = __shfl_down_sync(kFull, nR, d);
+            if (lane + d < 32) {
+                for (int c = 0; c < 3; ++c) { R[c] = fminf(R[c], t[c]); R[3 + c] = fmaxf(R[3 + c], t[3 + c]); }
+                nR += rn;
+            }
+        }
+        float Rn[6];
+        for (int c = 0; c < 6; ++c) Rn[c] = __shfl_down_sync(kFull, R[c], 1);
+        const int nRn = __shfl_down_sync(kFull, nR, 1);
+        if (lane < kSahBins - 1 && nL != 0 && nRn != 0) {
+            const Box3 lb = {{L[0], L[1], L[2]}, {L[3], L[4], L[5]}};
+            const Box3 rb = {{Rn[0], Rn[1], Rn[2]}, {Rn[3], Rn[4], Rn[5]}};
+            const float c = nL * half_area(lb) + nRn * half_area(rb);
+            if (c < best_c) { best_c = c; best_key = a * 32 + lane; best_nl = nL; }
+        }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        const float oc = __shfl_xor_sync(kFull, best_c, d);
+        const int ok = __shfl_xor_sync(kFull, best_key, d), onl = __shfl_xor_sync(kFull, best_nl, d);
+        if (oc < best_c || (oc == best_c && ok < best_key)) { best_c = oc; best_key = ok; best_nl = onl; }
+    }
+    if (best_key == 0x7fffffff) {
+        axis = -1; split = 0; nl = 0;
+    } else {
+        axis = best_key / 32; split = best_key % 32 + 1; nl = best_nl;
+    }
+}
+
+// The two sides' boxes of a split (sah_sides with a warp).
+__device__ __forceinline__ void warp_sides(const LaneBin& b, int lane, int split, Box3& l, Box3& r) {
+    for (int c = 0; c < 3; ++c) {
+        float llo = lane < split ? b.lo[c] : INFINITY, lhi = lane < split ? b.hi[c] : -INFINITY;
+        float rlo = lane < split ? INFINITY : b.lo[c], rhi = lane < split ? -INFINITY : b.hi[c];
+        for (int d = 16; d > 0; d >>= 1) {
+            llo = fminf(llo, __shfl_xor_sync(kFull, llo, d));
+            lhi = fmaxf(lhi, __shfl_xor_sync(kFull, lhi, d));
+            rlo = fminf(rlo, __shfl_xor_sync(kFull, rlo, d));
+            rhi = fmaxf(rhi, __shfl_xor_sync(kFull, rhi, d));
+        }
+        l.lo[c] = llo; l.hi[c] = lhi;
+        r.lo[c] = rlo; r.hi[c] = rhi;
     }
 }
 
@@ -215,12 +294,10 @@ __device__ __forceinline__ void push_child(const SahLevel& L, int node, uint32_t
     else L.next_small[atomicAdd(&L.ctr[1], 1)] = node;
 }
 
-// Records the split of node nd (first, count) at (axis, split) with nl on the left.
+// Records the split of node nd (first, count) with nl patches on the left.
 __device__ __forceinline__ void make_children(const SahLevel& L, int nd, uint32_t first, uint32_t count, uint32_t nl,
-                                              const SahBins& B, int axis, int split) {
+                                              const Box3& bl, const Box3& br) {
     const int l = atomicAdd(&L.ctr[2], 2), r = l + 1;
-    Box3 bl, br;
-    sah_sides(B, axis, split, bl, br);
     L.nbox[l] = bl;
     L.lf[l] = first;
     L.pc[l] = nl;
@@ -268,28 +345,23 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_sah_small(SahLevel L) {
         bins_add(B, L.prim[id], c, lo, ext, scale);
     }
     __syncwarp();
-    bins_decode(B, lane, 32);
-    __syncwarp();
-    int axis = -1, split = 0, nl = 0;
-    if (lane == 0) {
-        sah_choose(B.f, ext, axis, split);
-        if (axis >= 0)
-            for (int k = 0; k < split; ++k) nl += B.f.cnt[axis][k];
-    }
-    axis = __shfl_sync(kFull, axis, 0);
-    split = __shfl_sync(kFull, split, 0);
-    nl = __shfl_sync(kFull, nl, 0);
+    const LaneBin b[3] = {lane_bin(B, 0, lane), lane_bin(B, 1, lane), lane_bin(B, 2, lane)};
+    int axis, split, nl;
+    warp_choose(b, ext, lane, axis, split, nl);
     if (axis < 0 || nl == 0 || (uint32_t)nl == count) {  // all centroids coincide: a leaf
         if (lane == 0 && count > 8) atomicMax(&L.ctr[3], (int)count);
         return;
     }
+    Box3 bl, br;
+    warp_sides(b[axis], lane, split, bl, br);
+    const float alo = lo[axis], ascale = scale[axis];
     // stable partition through order2
     uint32_t lbase = 0;
     for (uint32_t i0 = 0; i0 < count; i0 += 32) {
         const uint32_t i = i0 + lane;
         const bool valid = i < count;
         const int id = valid ? L.order[first + i] : 0;
-        const bool left = valid && sah_bin(L.cen[3 * id + axis], lo[axis], scale[axis]) < split;
+        const bool left = valid && sah_bin(L.cen[3 * id + axis], alo, ascale) < split;
         const unsigned m = __ballot_sync(kFull, left);
         const uint32_t before = __popc(m & ((1u << lane) - 1u));
         if (valid) L.order2[first + (left ? lbase + before : nl + (i - lbase - before))] = id;
@@ -297,109 +369,243 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_sah_small(SahLevel L) {
     }
     __syncwarp();
     for (uint32_t i = lane; i < count; i += 32) L.order[first + i] = L.order2[first + i];
-    if (lane == 0) make_children(L, nd, first, count, (uint32_t)nl, B.f, axis, split);
+    if (lane == 0) make_children(L, nd, first, count, (uint32_t)nl, bl, br);
 }
 
-// A block per node (nodes of more than kBigNode patches); each warp fills its
-// own bins, merged before the split is chosen.
-__global__ void __launch_bounds__(kBigThreads) k_sah_big(SahLevel L) {
-    constexpr int NW = kBigThreads / 32;
-    extern __shared__ unsigned char smem[];
-    BinStore* wb = reinterpret_cast<BinStore*>(smem);  // NW per-warp bins, then the merged bins
-    BinStore& B = wb[NW];
-    __shared__ float red[6][NW];
-    __shared__ int sh_axis, sh_split, sh_nl;
-    __shared__ uint32_t wcount[NW];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nd = L.list[blockIdx.x];
-    const uint32_t first = L.lf[nd], count = L.pc[nd];
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t i = threadIdx.x; i < count; i += kBigThreads) {
-        const int id = L.order[first + i];
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = fminf(lo[a], L.cen[3 * id + a]);
-            hi[a] = fmaxf(hi[a], L.cen[3 * id + a]);
-        }
+// Nodes of more than kBigNode patches are cut into chunks of kChunk patches,
+// each handled by one block: bounds and bins meet in the node's state through
+// atomics, one warp per node chooses the split, and each chunk scatters its
+// patches after the left counts of the chunks before it (stable overall).
+constexpr int kChunk = 4096;
+constexpr int kChunkThreads = 256;
+
+struct BigState {
+    int bounds[6];   // centroid bounds, ordered ints: lo xyz, hi xyz
+    int axis, split, nl, nch;
+    uint32_t first, count;  // the node's patch range (its node record changes once it is split)
+    BinStore bins;
+};
+
+struct BigLevel {
+    SahLevel L;
+    BigState* st;
+    int* chunk_cnt;        // n_big + 1: chunks per node (last 0)
+    int* chunk_off;        // n_big + 1: first chunk of each node, [n_big] = total
+    int* chunk_left;       // per chunk: patches going left
+    int* chunk_pre;        // per chunk: left patches of the node's earlier chunks
+};
+
+// Node j and the patch range [b, e) of chunk c.
+__device__ __forceinline__ int chunk_range(const BigLevel& G, int c, uint32_t& b, uint32_t& e, uint32_t& first) {
+    const int j = find_owner(G.chunk_off, G.L.n_list, c);
+    first = G.st[j].first;
+    b = (uint32_t)(c - G.chunk_off[j]) * kChunk;
+    e = min(b + (uint32_t)kChunk, G.st[j].count);
+    return j;
+}
+
+__global__ void k_big_init(BigLevel G) {
+    const int j = blockIdx.x;
+    BigState& s = G.st[j];
+    bins_clear(s.bins, threadIdx.x, blockDim.x);
+    if (threadIdx.x < 3) {
+        s.bounds[threadIdx.x] = f2o(INFINITY);
+        s.bounds[3 + threadIdx.x] = f2o(-INFINITY);
     }
-    for (int o = 16; o > 0; o >>= 1)
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = fminf(lo[a], __shfl_xor_sync(kFull, lo[a], o));
-            hi[a] = fmaxf(hi[a], __shfl_xor_sync(kFull, hi[a], o));
-        }
-    if (lane == 0)
-        for (int a = 0; a < 3; ++a) { red[a][w] = lo[a]; red[3 + a][w] = hi[a]; }
-    bins_clear(wb[w], lane, 32);
-    __syncthreads();
-    for (int a = 0; a < 3; ++a) {
-        lo[a] = INFINITY;
-        hi[a] = -INFINITY;
-        for (int i = 0; i < NW; ++i) {
-            lo[a] = fminf(lo[a], red[a][i]);
-            hi[a] = fmaxf(hi[a], red[3 + a][i]);
-        }
+    if (threadIdx.x == 0) {
+        const int nd = G.L.list[j];
+        const uint32_t count = G.L.pc[nd];
+        s.first = G.L.lf[nd];
+        s.count = count;
+        s.nch = (int)((count + kChunk - 1) / kChunk);
+        G.chunk_cnt[j] = s.nch;
+        if (j == 0) G.chunk_cnt[G.L.n_list] = 0;
     }
-    float ext[3], scale[3];
+}
+
+__device__ __forceinline__ void node_frame(const BigState& s, float lo[3], float ext[3], float scale[3]) {
     for (int a = 0; a < 3; ++a) {
-        ext[a] = hi[a] - lo[a];
+        lo[a] = o2f(s.bounds[a]);
+        ext[a] = o2f(s.bounds[3 + a]) - lo[a];
         scale[a] = kSahBins / ext[a];
     }
-    for (uint32_t i = threadIdx.x; i < count; i += kBigThreads) {
-        const int id = L.order[first + i];
-        const float c[3] = {L.cen[3 * id], L.cen[3 * id + 1], L.cen[3 * id + 2]};
-        bins_add(wb[w], L.prim[id], c, lo, ext, scale);
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 3 * kSahBins; e += kBigThreads) {  // merge the warps' bins
-        const int a = e / kSahBins, k = e % kSahBins;
-        int cnt = 0, blo[3], bhi[3];
-        for (int c = 0; c < 3; ++c) { blo[c] = f2o(INFINITY); bhi[c] = f2o(-INFINITY); }
-        for (int i = 0; i < NW; ++i) {
-            cnt += wb[i].i.cnt[a][k];
-            for (int c = 0; c < 3; ++c) {
-                blo[c] = min(blo[c], wb[i].i.lo[a][k][c]);
-                bhi[c] = max(bhi[c], wb[i].i.hi[a][k][c]);
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_big_bounds(BigLevel G) {
+    __shared__ float red[6][kChunkThreads / 32];
+    const int total = G.chunk_off[G.L.n_list];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        uint32_t b, e, first;
+        const int j = chunk_range(G, c, b, e, first);
+        float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t i = b + threadIdx.x; i < e; i += kChunkThreads) {
+            const int id = G.L.order[first + i];
+            for (int a = 0; a < 3; ++a) {
+                v[a] = fminf(v[a], G.L.cen[3 * id + a]);
+                v[3 + a] = fmaxf(v[3 + a], G.L.cen[3 * id + a]);
             }
         }
-        B.f.cnt[a][k] = cnt;
-        for (int c = 0; c < 3; ++c) { B.f.lo[a][k][c] = o2f(blo[c]); B.f.hi[a][k][c] = o2f(bhi[c]); }
+        for (int o = 16; o > 0; o >>= 1)
+            for (int a = 0; a < 3; ++a) {
+                v[a] = fminf(v[a], __shfl_xor_sync(kFull, v[a], o));
+                v[3 + a] = fmaxf(v[3 + a], __shfl_xor_sync(kFull, v[3 + a], o));
+            }
+        if (lane == 0)
+            for (int a = 0; a < 6; ++a) red[a][w] = v[a];
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            const int a = threadIdx.x;
+            float r = red[a][0];
+            for (int k = 1; k < kChunkThreads / 32; ++k) r = a < 3 ? fminf(r, red[a][k]) : fmaxf(r, red[a][k]);
+            if (r == r) {  // an all-NaN chunk adds nothing
+                if (a < 3) atomicMin(&G.st[j].bounds[a], f2o(r));
+                else atomicMax(&G.st[j].bounds[a], f2o(r));
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int axis, split, nl = 0;
-        sah_choose(B.f, ext, axis, split);
-        if (axis >= 0)
-            for (int k = 0; k < split; ++k) nl += B.f.cnt[axis][k];
-        sh_axis = axis;
-        sh_split = split;
-        sh_nl = nl;
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_big_bins(BigLevel G) {
+    __shared__ BinStore B;
+    const int total = G.chunk_off[G.L.n_list];
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        uint32_t b, e, first;
+        const int j = chunk_range(G, c, b, e, first);
+        float lo[3], ext[3], scale[3];
+        node_frame(G.st[j], lo, ext, scale);
+        bins_clear(B, threadIdx.x, kChunkThreads);
+        __syncthreads();
+        for (uint32_t i = b + threadIdx.x; i < e; i += kChunkThreads) {
+            const int id = G.L.order[first + i];
+            const float cc[3] = {G.L.cen[3 * id], G.L.cen[3 * id + 1], G.L.cen[3 * id + 2]};
+            bins_add(B, G.L.prim[id], cc, lo, ext, scale);
+        }
+        __syncthreads();
+        BinStore& S = G.st[j].bins;
+        for (int t = threadIdx.x; t < 3 * kSahBins; t += kChunkThreads) {
+            const int a = t / kSahBins, k = t % kSahBins;
+            if (B.i.cnt[a][k] == 0) continue;
+            atomicAdd(&S.i.cnt[a][k], B.i.cnt[a][k]);
+            for (int d = 0; d < 3; ++d) {
+                atomicMin(&S.i.lo[a][k][d], B.i.lo[a][k][d]);
+                atomicMax(&S.i.hi[a][k][d], B.i.hi[a][k][d]);
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    const int axis = sh_axis, split = sh_split;
-    const uint32_t nl = (uint32_t)sh_nl;
-    if (axis < 0 || nl == 0 || nl == count) {
-        if (threadIdx.x == 0 && count > 8) atomicMax(&L.ctr[3], (int)count);
+}
+
+// A warp per big node: the split, the children, the chunks' left-count prefix
+// comes later (k_big_prefix).
+__global__ void k_big_choose(BigLevel G) {
+    const int j = blockIdx.x, lane = threadIdx.x;
+    BigState& s = G.st[j];
+    const int nd = G.L.list[j];
+    const uint32_t first = s.first, count = s.count;
+    float lo[3], ext[3], scale[3];
+    node_frame(s, lo, ext, scale);
+    const LaneBin b[3] = {lane_bin(s.bins, 0, lane), lane_bin(s.bins, 1, lane), lane_bin(s.bins, 2, lane)};
+    int axis, split, nl;
+    warp_choose(b, ext, lane, axis, split, nl);
+    if (axis < 0 || nl == 0 || (uint32_t)nl == count) {
+        if (lane == 0) {
+            s.axis = -1;
+            if (count > 8) atomicMax(&G.L.ctr[3], (int)count);
+        }
         return;
     }
-    uint32_t lbase = 0;
-    for (uint32_t i0 = 0; i0 < count; i0 += kBigThreads) {
-        const uint32_t i = i0 + threadIdx.x;
-        const bool valid = i < count;
-        const int id = valid ? L.order[first + i] : 0;
-        const bool left = valid && sah_bin(L.cen[3 * id + axis], lo[axis], scale[axis]) < split;
-        const unsigned m = __ballot_sync(kFull, left);
-        if (lane == 0) wcount[w] = __popc(m);
-        __syncthreads();
-        uint32_t before = __popc(m & ((1u << lane) - 1u)), total = 0;
-        for (int j = 0; j < NW; ++j) {
-            if (j < w) before += wcount[j];
-            total += wcount[j];
+    Box3 bl, br;
+    warp_sides(b[axis], lane, split, bl, br);
+    if (lane == 0) {
+        s.axis = axis;
+        s.split = split;
+        s.nl = nl;
+        make_children(G.L, nd, first, count, (uint32_t)nl, bl, br);
+    }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_big_count(BigLevel G) {
+    __shared__ int red[kChunkThreads / 32];
+    const int total = G.chunk_off[G.L.n_list];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        uint32_t b, e, first;
+        const int j = chunk_range(G, c, b, e, first);
+        const BigState& s = G.st[j];
+        if (s.axis < 0) continue;  // uniform over the block
+        float lo[3], ext[3], scale[3];
+        node_frame(s, lo, ext, scale);
+        int n = 0;
+        for (uint32_t i = b + threadIdx.x; i < e; i += kChunkThreads) {
+            const int id = G.L.order[first + i];
+            n += sah_bin(G.L.cen[3 * id + s.axis], lo[s.axis], scale[s.axis]) < s.split;
         }
-        if (valid) L.order2[first + (left ? lbase + before : nl + (i - lbase - before))] = id;
-        lbase += total;
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(kFull, n, o);
+        if (lane == 0) red[w] = n;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int k = 0; k < kChunkThreads / 32; ++k) t += red[k];
+            G.chunk_left[c] = t;
+        }
         __syncthreads();
     }
-    for (uint32_t i = threadIdx.x; i < count; i += kBigThreads) L.order[first + i] = L.order2[first + i];
-    if (threadIdx.x == 0) make_children(L, nd, first, count, nl, B.f, axis, split);
+}
+
+__global__ void k_big_prefix(BigLevel G) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= G.L.n_list || G.st[j].axis < 0) return;
+    int acc = 0;
+    for (int c = G.chunk_off[j]; c < G.chunk_off[j + 1]; ++c) {
+        G.chunk_pre[c] = acc;
+        acc += G.chunk_left[c];
+    }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_big_scatter(BigLevel G) {
+    constexpr int NW = kChunkThreads / 32;
+    __shared__ uint32_t wcount[NW];
+    const int total = G.chunk_off[G.L.n_list];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        uint32_t b, e, first;
+        const int j = chunk_range(G, c, b, e, first);
+        const BigState& s = G.st[j];
+        if (s.axis < 0) continue;
+        float lo[3], ext[3], scale[3];
+        node_frame(s, lo, ext, scale);
+        const uint32_t nl = (uint32_t)s.nl;
+        uint32_t lbase = (uint32_t)G.chunk_pre[c];  // left patches before this position in the node
+        for (uint32_t i0 = b; i0 < e; i0 += kChunkThreads) {
+            const uint32_t i = i0 + threadIdx.x;
+            const bool valid = i < e;
+            const int id = valid ? G.L.order[first + i] : 0;
+            const bool left = valid && sah_bin(G.L.cen[3 * id + s.axis], lo[s.axis], scale[s.axis]) < s.split;
+            const unsigned m = __ballot_sync(kFull, left);
+            if (lane == 0) wcount[w] = __popc(m);
+            __syncthreads();
+            uint32_t before = __popc(m & ((1u << lane) - 1u)), tot = 0;
+            for (int k = 0; k < NW; ++k) {
+                if (k < w) before += wcount[k];
+                tot += wcount[k];
+            }
+            if (valid) G.L.order2[first + (left ? lbase + before : nl + (i - lbase - before))] = id;
+            lbase += tot;
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_big_copy(BigLevel G) {
+    const int total = G.chunk_off[G.L.n_list];
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        uint32_t b, e, first;
+        const int j = chunk_range(G, c, b, e, first);
+        if (G.st[j].axis < 0) continue;
+        for (uint32_t i = b + threadIdx.x; i < e; i += kChunkThreads) G.L.order[first + i] = G.L.order2[first + i];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -516,6 +722,24 @@ __global__ void k_rank_of(const int32_t* __restrict__ by_rank, int N, int32_t* r
 // ---------------------------------------------------------------------------
 // Host side
 
+// f(i) for i in [0, n) on up to 16 threads (inline for small n).
+template <class F>
+void parallel_for(int n, F f) {
+    const int T = (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (n < 32 || T == 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    auto work = [&] {
+        for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) f(i);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+}
+
 unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 // Scratch carved from one allocation, 256-byte aligned pieces.
@@ -545,13 +769,16 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
     cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
                                     (const int32_t*)nullptr, (int32_t*)nullptr, N, 0, 8);
     const size_t tmp_bytes = std::max(scan_bytes, sort_bytes);
+    const size_t cap_big = (size_t)N / kBigNode + 2, cap_chunks = (size_t)N / kChunk + cap_big + 2;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t need = al(N * sizeof(Box3)) + al(3 * (size_t)N * sizeof(float)) + 2 * al(N * sizeof(int32_t)) +
                         al(M * sizeof(Box3)) + 2 * al(M * sizeof(uint32_t)) + 4 * al((N + 1) * sizeof(int32_t)) +
                         al(8 * sizeof(int)) + al((N + 1) * sizeof(Node4)) + al((N + 1) * sizeof(uint32_t)) +
                         al(4 * (size_t)(N + 1) * sizeof(uint32_t)) + 2 * al((N + 2) * sizeof(int)) +
                         2 * al((N + 1) * sizeof(long long)) + 2 * al(N * sizeof(uint32_t)) +
-                        2 * al(N * sizeof(int32_t)) + al(64 * sizeof(int)) + al(tmp_bytes) + 256;
+                        2 * al(N * sizeof(int32_t)) + al(64 * sizeof(int)) + al(tmp_bytes) +
+                        al(cap_big * sizeof(BigState)) + 2 * al((cap_big + 1) * sizeof(int)) +
+                        2 * al(cap_chunks * sizeof(int)) + 256;
     Scratch S;
     cudaError_t e = cudaMalloc(&S.base, need);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(scene build scratch)");
@@ -583,6 +810,11 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
     int32_t* by_rank = S.take<int32_t>(N);
     int* hist = S.take<int>(64);
     void* tmp = S.take<char>(tmp_bytes);
+    BigState* big = S.take<BigState>(cap_big);
+    int* chunk_cnt = S.take<int>(cap_big + 1);
+    int* chunk_off = S.take<int>(cap_big + 1);
+    int* chunk_left = S.take<int>(cap_chunks);
+    int* chunk_pre = S.take<int>(cap_chunks);
     auto check = [&](const char* what) -> int {
         const cudaError_t k = cudaGetLastError();
         return k == cudaSuccess ? NRT_OK : cuda_fail(k, what);
@@ -604,9 +836,6 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
         else { cudaMemcpy(lists[1], &root, sizeof(root), cudaMemcpyHostToDevice); n_small = 1; }
     }
     cudaMemcpy(ctr, h_ctr, sizeof(h_ctr), cudaMemcpyHostToDevice);
-    const size_t big_smem = (kBigThreads / 32 + 1) * sizeof(BinStore);
-    e = cudaFuncSetAttribute(k_sah_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_sah_big)");
     int cur = 0;
     while (n_big + n_small > 0) {
         cudaMemset(ctr, 0, 2 * sizeof(int));
@@ -615,7 +844,19 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
         if (n_big) {
             L.list = lists[2 * cur];
             L.n_list = n_big;
-            k_sah_big<<<n_big, kBigThreads, big_smem>>>(L);
+            const BigLevel G{L, big, chunk_cnt, chunk_off, chunk_left, chunk_pre};
+            k_big_init<<<n_big, 128>>>(G);
+            size_t tb = tmp_bytes;
+            e = cub::DeviceScan::ExclusiveSum(tmp, tb, chunk_cnt, chunk_off, n_big + 1);
+            if (e != cudaSuccess) return cuda_fail(e, "scene build: chunk scan");
+            const unsigned grid = (unsigned)std::min<long long>(148 * 4, (long long)N / kChunk + n_big + 1);
+            k_big_bounds<<<grid, kChunkThreads>>>(G);
+            k_big_bins<<<grid, kChunkThreads>>>(G);
+            k_big_choose<<<n_big, 32>>>(G);
+            k_big_count<<<grid, kChunkThreads>>>(G);
+            k_big_prefix<<<blocks_for(n_big, 128), 128>>>(G);
+            k_big_scatter<<<grid, kChunkThreads>>>(G);
+            k_big_copy<<<grid, kChunkThreads>>>(G);
         }
         if (n_small) {
             L.list = lists[2 * cur + 1];
@@ -726,17 +967,25 @@ int build_scene_device_surfaces(const nrt_nurbs_surface* surfaces, int n_surface
     PatchSet ps;
     long long pts_net = 0, pts_strip = 0, pts_cp = 0, n_knots = 0, n_floats = 0, lines_u = 0, lines_v = 0;
     long long N = 0;
-    std::vector<float> bu, bv;
+    ps.spans.resize(n_surfaces);
     for (int si = 0; si < n_surfaces; ++si) {
         const nrt_nurbs_surface& s = surfaces[si];
         if (int st = check_surface(s)) {
             set_error("surface %d: %s", si, nrt_last_error());
             return st;
         }
-        bu.resize(s.n - s.p + 2);
-        bv.resize(s.m - s.q + 2);
-        const int nbU = knot_spans(s.u_knots, s.n + s.p + 1, s.p, bu.data());
-        const int nbV = knot_spans(s.v_knots, s.m + s.q + 1, s.q, bv.data());
+        PatchSet::Spans& sp = ps.spans[si];
+        sp.bu = ps.breaks.size();
+        ps.breaks.resize(sp.bu + (s.n - s.p + 2));
+        const int nbU = knot_spans(s.u_knots, s.n + s.p + 1, s.p, &ps.breaks[sp.bu]);
+        ps.breaks.resize(sp.bu + nbU + 1);
+        sp.bv = ps.breaks.size();
+        ps.breaks.resize(sp.bv + (s.m - s.q + 2));
+        const int nbV = knot_spans(s.v_knots, s.m + s.q + 1, s.q, &ps.breaks[sp.bv]);
+        ps.breaks.resize(sp.bv + nbV + 1);
+        sp.patch0 = (int)N;
+        sp.nbU = nbU;
+        sp.nbV = nbV;
         SurfDesc& d = sd[si];
         d.n = s.n; d.m = s.m; d.p = s.p; d.q = s.q; d.nbU = nbU; d.nbV = nbV;
         d.net = pts_net;
@@ -760,27 +1009,24 @@ int build_scene_device_surfaces(const nrt_nurbs_surface* surfaces, int n_surface
         N += (long long)nbU * nbV;
         if (N >= (1 << 27) || lines_u >= (1LL << 31) || lines_v >= (1LL << 31))
             return fail(NRT_ERR_INVALID, "too many patches");
-        for (int i = 0; i < nbU; ++i)
-            for (int j = 0; j < nbV; ++j) {
-                ps.ranges.insert(ps.ranges.end(), {bu[i], bu[i + 1], bv[j], bv[j + 1]});
-                ps.surf.push_back(si);
-            }
     }
     if (n_floats >= (1LL << 31)) return fail(NRT_ERR_INVALID, "scene too large (%lld block floats)", n_floats);
-    // nets and knots, packed on the host and copied once
-    std::vector<P4> nets((size_t)pts_net);
-    std::vector<float> knots((size_t)n_knots);
-    for (int si = 0; si < n_surfaces; ++si) {
+    // nets and knots, packed on the host (several threads: the first touch of
+    // fresh pages dominates) and copied once
+    std::unique_ptr<P4[]> nets(new (std::nothrow) P4[(size_t)pts_net]);
+    std::unique_ptr<float[]> knots(new (std::nothrow) float[(size_t)n_knots]);
+    if (!nets || !knots) return fail(NRT_ERR_NOMEM, "host allocation failed");
+    parallel_for(n_surfaces, [&](int si) {
         const nrt_nurbs_surface& s = surfaces[si];
         const SurfDesc& d = sd[si];
         std::memcpy(&nets[d.net], s.control_points, sizeof(P4) * (size_t)(s.n + 1) * (s.m + 1));
         std::memcpy(&knots[d.ku], s.u_knots, sizeof(float) * (s.n + s.p + 2));
         std::memcpy(&knots[d.kv], s.v_knots, sizeof(float) * (s.m + s.q + 2));
-    }
+    });
     DeviceGuard dg(o.device);
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t need = al(sd.size() * sizeof(SurfDesc)) + 3 * al(n_surfaces * sizeof(int)) +
-                        al(nets.size() * sizeof(P4)) + al(knots.size() * sizeof(float)) +
+                        al((size_t)pts_net * sizeof(P4)) + al((size_t)n_knots * sizeof(float)) +
                         al((size_t)pts_strip * sizeof(P4)) + al((size_t)pts_cp * sizeof(P4)) +
                         al((size_t)N * sizeof(long long)) + al(2 * (size_t)N * sizeof(int)) +
                         al((size_t)N * sizeof(int)) + al(sizeof(int)) + 256;
@@ -795,8 +1041,8 @@ int build_scene_device_surfaces(const nrt_nurbs_surface* surfaces, int n_surface
     int* d_line_u = S.take<int>(n_surfaces);
     int* d_line_v = S.take<int>(n_surfaces);
     int* d_patch0 = S.take<int>(n_surfaces);
-    P4* d_nets = S.take<P4>(nets.size());
-    float* d_knots = S.take<float>(knots.size());
+    P4* d_nets = S.take<P4>((size_t)pts_net);
+    float* d_knots = S.take<float>((size_t)n_knots);
     P4* d_strips = S.take<P4>((size_t)pts_strip);
     P4* d_cp = S.take<P4>((size_t)pts_cp);
     long long* d_off = S.take<long long>((size_t)N);
@@ -807,8 +1053,8 @@ int build_scene_device_surfaces(const nrt_nurbs_surface* surfaces, int n_surface
     if (e == cudaSuccess) e = cudaMemcpy(d_line_u, line_u.data(), n_surfaces * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_line_v, line_v.data(), n_surfaces * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_patch0, patch0.data(), n_surfaces * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_nets, nets.data(), nets.size() * sizeof(P4), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_knots, knots.data(), knots.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_nets, nets.get(), (size_t)pts_net * sizeof(P4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_knots, knots.get(), (size_t)n_knots * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_err, 0, sizeof(int));
     if (e != cudaSuccess) return cuda_fail(e, "scene build: upload");
     k_split_u<<<blocks_for(lines_u, 128), 128>>>(d_sd, d_line_u, n_surfaces, (int)lines_u, d_nets, d_knots, d_strips,
