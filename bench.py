@@ -178,6 +178,44 @@ def cpu_reference_rate(scene_def, rays_np, seconds=10.0, iters=8, eps=1e-6, port
                       f"(midpoint init, {iters} evaluations, eps {eps:g})"}
 
 
+def scene_build_block(torch, nrt, scenes):
+    """Scene creation (decomposition, BVH, packing, upload) on the device
+    (NRT_BVH_BINNED_SAH_DEVICE) and on the host (NRT_BVH_BINNED_SAH), wall
+    clock around the synchronous call; the two arenas are compared byte for
+    byte (signed zeros aside)."""
+    import numpy as np
+
+    bsc = scenes.surfaces_grid_scene(256, 11, 64, 64, 1, net_range=(64, 96), name="big256")
+
+    def build(builder):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s = nrt.Scene(bsc.surfaces, builder=builder)
+        torch.cuda.synchronize()
+        return s, time.perf_counter() - t0
+
+    dev_s = []
+    for _ in range(4):  # the first call loads the module and warms the allocator
+        s, dt = build(nrt.BVH_BINNED_SAH_DEVICE)
+        dev_s.append(dt)
+        a_dev = s.arena()
+        info = s.info()
+        s.close()
+    s, host_s = build(nrt.BVH_BINNED_SAH)
+    a_host = s.arena()
+    s.close()
+    wa, wb = a_dev.view(np.uint32), a_host.view(np.uint32)
+    d = wa != wb
+    signed_zero = ((wa[d] | wb[d]) == 0x80000000) & ((wa[d] & wb[d]) == 0)
+    dev_ms = 1e3 * min(dev_s[1:])
+    return {"workload": f"256 random NURBS surfaces deg 2-5, nets 64-96 ({info['n_patches']} Bezier patches, "
+                        f"{info['n_nodes']} BVH nodes)",
+            "device_ms": round(dev_ms, 2), "host_ms": round(1e3 * host_s, 1),
+            "speedup": round(host_s * 1e3 / dev_ms, 1), "device_Mpatches_per_s": round(info["n_patches"] / dev_ms / 1e3, 2),
+            "arena_identical": bool(signed_zero.all()), "arena_bytes": int(a_dev.size),
+            "note": "wall clock of nrt_scene_create (min of 3 after a warm-up; host: one call)"}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -424,6 +462,14 @@ def nrt_arm(args):
         except Exception as exc:  # reported, never silently replaced
             bounce_block = {"error": str(exc)[:200]}
 
+    # scene build, device vs host, on 256 large surfaces (668,919 Bezier patches); rank 0 only
+    build_block = None
+    if rank == 0 and not args.no_scene_build:
+        try:
+            build_block = scene_build_block(torch, nrt, scenes)
+        except Exception as exc:  # reported, never silently replaced
+            build_block = {"error": str(exc)[:200]}
+
     line = None
     if rank == 0:
         nl = max(1, kt["newton_kernel_launches"])
@@ -472,6 +518,7 @@ def nrt_arm(args):
                 "learned_init_wavefront": learned_block,
                 "precision_stress": prec_block,
                 "bounce_batches": bounce_block,
+                "scene_build": build_block,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 24 * n,
                         "d2h_bytes_per_step": 16 * n},
@@ -489,6 +536,8 @@ def main():
     ap.add_argument("--impl", default="nrt", choices=["nrt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bounce", action="store_true", help="skip the 256-surface bounce-batch measurement")
+    ap.add_argument("--no-scene-build", action="store_true",
+                    help="skip the device-vs-host scene build measurement (669k patches)")
     ap.add_argument("--profile", action="store_true", help="only launch the timed kernels (for ncu)")
     ap.add_argument("--profile-plain", action="store_true", help="with --profile: the plain per-pixel path")
     ap.add_argument("--spp", type=int, default=4,
