@@ -97,40 +97,61 @@ __device__ __forceinline__ PatchRay patch_ray(const RayFrame& r, double cx, doub
     return pr;
 }
 
-// Tensor-product rational Bezier evaluation of one homogeneous coordinate:
-// every row (along v) is reduced by de Casteljau to two points, giving the
-// row point at v and its v-derivative; the row points are reduced along u to
-// two points (value and u-derivative) and the v-derivatives to one point.
-// This yields H, dH/du, dH/dv with (p+1)q(q+1)/2 + p(p+1) lerps, against the
-// two full passes of BezierPatchEval (src/math/bezier_patch.h:172-191).
+// Bernstein values of degree N at t, B[i] = C(N,i) t^i (1-t)^(N-i), and their
+// derivatives dB[i] = N (B^{N-1}[i-1] - B^{N-1}[i]), from the degree N-1
+// values built by the triangle recursion b_i <- (1-t) b_i + t b_{i-1}.
+template <int N, class T>
+__device__ __forceinline__ void bernstein(T t, T (&B)[N + 1], T (&dB)[N + 1]) {
+    const T s = T(1) - t;
+    T b[N];
+    b[0] = T(1);
+#pragma unroll
+    for (int k = 1; k < N; ++k) {  // degree k from degree k-1, in place from the top
+        b[k] = t * b[k - 1];
+#pragma unroll
+        for (int i = k - 1; i >= 1; --i) b[i] = fmx(s, b[i], t * b[i - 1]);
+        b[0] = s * b[0];
+    }
+    B[0] = s * b[0];
+    B[N] = t * b[N - 1];
+    dB[0] = -T(N) * b[0];
+    dB[N] = T(N) * b[N - 1];
+#pragma unroll
+    for (int i = 1; i < N; ++i) {
+        B[i] = fmx(s, b[i], t * b[i - 1]);
+        dB[i] = T(N) * (b[i - 1] - b[i]);
+    }
+}
+
+// Tensor-product rational Bezier evaluation of one homogeneous coordinate as
+// a Bernstein sum: each row i is summed along v with the basis values and
+// their derivatives (the row point and its v-derivative), then the rows are
+// summed along u.  H, dH/du, dH/dv cost 2(p+1)(q+1) + 3(p+1) multiply-adds,
+// with the basis values computed once per (u, v) for all four coordinates;
+// the reference's BezierPatchEval (src/math/bezier_patch.h:172-191) runs two
+// full de Casteljau passes instead.
 template <int P, int Q, class T>
-__device__ __forceinline__ void eval_coord(const T (&c)[(P + 1) * (Q + 1)], T u, T v, T& h, T& hu, T& hv) {
-    T pt[P + 1], dv[P + 1];
+__device__ __forceinline__ void eval_coord(const T (&c)[(P + 1) * (Q + 1)], const T (&Bu)[P + 1],
+                                           const T (&dBu)[P + 1], const T (&Bv)[Q + 1], const T (&dBv)[Q + 1], T& h,
+                                           T& hu, T& hv) {
 #pragma unroll
     for (int i = 0; i <= P; ++i) {
-        T r[Q + 1];
+        T r = Bv[0] * c[i * (Q + 1)], d = dBv[0] * c[i * (Q + 1)];
 #pragma unroll
-        for (int j = 0; j <= Q; ++j) r[j] = c[i * (Q + 1) + j];
-#pragma unroll
-        for (int k = 1; k < Q; ++k)
-#pragma unroll
-            for (int j = 0; j <= Q - k; ++j) r[j] = fmx(v, r[j + 1] - r[j], r[j]);
-        const T dl = r[1] - r[0];
-        pt[i] = fmx(v, dl, r[0]);
-        dv[i] = T(Q) * dl;
+        for (int j = 1; j <= Q; ++j) {
+            r = fmx(Bv[j], c[i * (Q + 1) + j], r);
+            d = fmx(dBv[j], c[i * (Q + 1) + j], d);
+        }
+        if (i == 0) {
+            h = Bu[0] * r;
+            hu = dBu[0] * r;
+            hv = Bu[0] * d;
+        } else {
+            h = fmx(Bu[i], r, h);
+            hu = fmx(dBu[i], r, hu);
+            hv = fmx(Bu[i], d, hv);
+        }
     }
-#pragma unroll
-    for (int k = 1; k < P; ++k)
-#pragma unroll
-        for (int i = 0; i <= P - k; ++i) pt[i] = fmx(u, pt[i + 1] - pt[i], pt[i]);
-#pragma unroll
-    for (int k = 1; k <= P; ++k)
-#pragma unroll
-        for (int i = 0; i <= P - k; ++i) dv[i] = fmx(u, dv[i + 1] - dv[i], dv[i]);
-    const T dl = pt[1] - pt[0];
-    h = fmx(u, dl, pt[0]);
-    hu = T(P) * dl;
-    hv = dv[0];
 }
 
 // Load one coordinate array of a patch block with 16-byte loads.
@@ -153,11 +174,14 @@ template <int P, int Q, class T>
 __device__ __forceinline__ void eval_patch(const float* __restrict__ blk, T u, T v, T (&H)[4], T (&Hu)[4],
                                            T (&Hv)[4]) {
     constexpr int NP = padded_points(P, Q);
+    T Bu[P + 1], dBu[P + 1], Bv[Q + 1], dBv[Q + 1];
+    bernstein<P, T>(u, Bu, dBu);
+    bernstein<Q, T>(v, Bv, dBv);
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         T c[(P + 1) * (Q + 1)];
         load_coord<P, Q, T>(blk + a * NP, c);
-        eval_coord<P, Q, T>(c, u, v, H[a], Hu[a], Hv[a]);
+        eval_coord<P, Q, T>(c, Bu, dBu, Bv, dBv, H[a], Hu[a], Hv[a]);
     }
 }
 
