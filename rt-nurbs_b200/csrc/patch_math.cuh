@@ -646,12 +646,16 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
         const float j21 = r.n2x * ux + r.n2y * uy + r.n2z * uz;
         const float j12 = r.n1x * vx + r.n1y * vy + r.n1z * vz;
         const float j22 = r.n2x * vx + r.n2y * vy + r.n2z * vz;
-        seed = pcg_hash(seed);
-        const float rnd1 = (float)seed * 2.3283064e-10f;
-        seed = pcg_hash(seed);
-        const float rnd2 = (float)seed * 2.3283064e-10f;
         const float det = j11 * j22 - j12 * j21;
         if (fabsf(det) < op.det_eps) {
+            // the reference advances the seed twice every iteration; the pull of
+            // iteration `it` uses its (2 it - 1)-th and (2 it)-th hashes, formed
+            // here only when they are needed
+            uint32_t s = seed;
+            for (int k = 1; k < 2 * it; ++k) s = pcg_hash(s);
+            const float rnd1 = (float)s * 2.3283064e-10f;
+            s = pcg_hash(s);
+            const float rnd2 = (float)s * 2.3283064e-10f;
             u = u + 0.1f * ((u0 - u) * rnd1);
             v = v + 0.1f * ((v0 - v) * rnd2);
         } else if (op.cond_fp64 > 0.f &&

@@ -823,8 +823,9 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
     // boxes, centroids, root
     k_boxes<<<blocks_for(N, 256), 256>>>(cp, off, deg, N, box, cen, order);
     k_root_box<<<1, 1024>>>(box, N, nbox);
-    cudaMemset(lf, 0, sizeof(uint32_t));
-    cudaMemcpy(pc, &N, sizeof(uint32_t), cudaMemcpyHostToDevice);
+    e = cudaMemset(lf, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(pc, &N, sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "scene build: root");
     if (int st = check("scene build: boxes")) return st;
 
     // binned SAH, a level at a time
@@ -832,13 +833,17 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
     int n_big = 0, n_small = 0;
     const int32_t root = 0;
     if (N > o.max_leaf) {
-        if (N > kBigNode) { cudaMemcpy(lists[0], &root, sizeof(root), cudaMemcpyHostToDevice); n_big = 1; }
-        else { cudaMemcpy(lists[1], &root, sizeof(root), cudaMemcpyHostToDevice); n_small = 1; }
+        if (N > kBigNode) n_big = 1;
+        else n_small = 1;
+        e = cudaMemcpy(lists[n_big ? 0 : 1], &root, sizeof(root), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "scene build: SAH root");
     }
-    cudaMemcpy(ctr, h_ctr, sizeof(h_ctr), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(ctr, h_ctr, sizeof(h_ctr), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "scene build: SAH counters");
     int cur = 0;
     while (n_big + n_small > 0) {
-        cudaMemset(ctr, 0, 2 * sizeof(int));
+        e = cudaMemset(ctr, 0, 2 * sizeof(int));
+        if (e != cudaSuccess) return cuda_fail(e, "scene build: SAH level");
         SahLevel L{box, cen, order, order2, nbox, lf, pc, nullptr, 0, lists[2 * (cur ^ 1)], lists[2 * (cur ^ 1) + 1],
                    ctr, o.max_leaf};
         if (n_big) {
@@ -873,7 +878,8 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
 
     // 4-wide collapse, breadth first
     const uint32_t zero = 0;
-    cudaMemcpy(queue, &zero, sizeof(zero), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(queue, &zero, sizeof(zero), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "scene build: collapse");
     int lb = 0, le = 1, depth = 0;
     while (le > lb) {
         const int n = le - lb;
@@ -911,7 +917,8 @@ int build_from_device_patches(const nrt_build_opts& o, int N, int n_surfaces, co
     };
     e = cudaMemcpy(base + A.nodes, wide, n_wide * sizeof(Node4), cudaMemcpyDeviceToDevice);
     if (e != cudaSuccess) return fail_scene(e, "scene build: nodes");
-    cudaMemset(hist, 0, 64 * sizeof(int));
+    e = cudaMemset(hist, 0, 64 * sizeof(int));
+    if (e != cudaSuccess) return fail_scene(e, "scene build: packing");
     PackOut po{reinterpret_cast<float*>(base + A.cp), reinterpret_cast<int4*>(base + A.hdr),
                reinterpret_cast<double4*>(base + A.centre), reinterpret_cast<float4*>(base + A.corners),
                reinterpret_cast<float*>(base + A.delta), reinterpret_cast<dev::PatchFrame*>(base + A.frames),
