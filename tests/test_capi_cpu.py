@@ -137,3 +137,100 @@ def test_invalid_inputs_report_errors(nrt_mod):
     with pytest.raises(nrt_mod.NrtError, match="clamped"):
         nrt_mod.decompose(scenes.Surface(s.cp, U, s.V, s.n, s.m, s.p, s.q))
     assert nrt_mod.lib().nrt_decompose(None, None, None, None, None) == 1
+
+
+def _binned_sah_restated(boxes, max_leaf=1):
+    """The 32-bin SAH as the builders define it (csrc/scene_math.h), restated
+    in numpy float32, one rounding per operation: centroid bounds, bins per
+    axis with a positive extent, cost nL*halfArea(L) + nR*halfArea(R) with the
+    first minimum in (axis, bin) order, a stable partition, children numbered
+    as a depth-first stack allocates them."""
+    f = np.float32
+    N = boxes.shape[0]
+    lo, hi = boxes[:, :3].astype(f), boxes[:, 3:].astype(f)
+    cen = (f(0.5) * (lo + hi)).astype(f)
+
+    def half_area(b_lo, b_hi):
+        ex, ey, ez = f(b_hi[0] - b_lo[0]), f(b_hi[1] - b_lo[1]), f(b_hi[2] - b_lo[2])
+        return f(f(f(ex * ey) + f(ey * ez)) + f(ez * ex))
+
+    def sah_bin(c, l, s):
+        v = f(f(c - l) * s)
+        return (int(v) if v < f(32) else 31) if v >= f(0) else 0
+
+    M = 2 * N - 1
+    nb = np.zeros((M, 6), f)
+    lf = np.zeros(M, np.uint32)
+    cnt = np.zeros(M, np.uint32)
+    order = np.arange(N, dtype=np.int32)
+    nb[0, :3], nb[0, 3:] = lo.min(0), hi.max(0)
+    cnt[0] = N
+    used, todo = 1, [0]
+    while todo:
+        node = todo.pop()
+        first, count = int(lf[node]), int(cnt[node])
+        if count <= max_leaf:
+            continue
+        ids = order[first:first + count]
+        clo, chi = cen[ids].min(0), cen[ids].max(0)
+        ext = (chi - clo).astype(f)
+        scale = [f(f(32) / ext[a]) if ext[a] > 0 else f(0) for a in range(3)]
+        best = (np.inf, -1, 0)
+        bins = {}
+        for a in range(3):
+            if not ext[a] > 0:
+                continue
+            bl = np.full((32, 3), np.inf, f); bh = np.full((32, 3), -np.inf, f); bc = np.zeros(32, int)
+            for i in ids:
+                b = sah_bin(cen[i, a], clo[a], scale[a])
+                bc[b] += 1; bl[b] = np.minimum(bl[b], lo[i]); bh[b] = np.maximum(bh[b], hi[i])
+            bins[a] = (bl, bh, bc)
+            rlo, rhi, n = np.full(3, np.inf, f), np.full(3, -np.inf, f), 0
+            ra, rc = [None] * 32, [0] * 32
+            for k in range(31, 0, -1):
+                rlo, rhi, n = np.minimum(rlo, bl[k]), np.maximum(rhi, bh[k]), n + bc[k]
+                ra[k], rc[k] = half_area(rlo, rhi), n
+            llo, lhi, n = np.full(3, np.inf, f), np.full(3, -np.inf, f), 0
+            for k in range(31):
+                llo, lhi, n = np.minimum(llo, bl[k]), np.maximum(lhi, bh[k]), n + bc[k]
+                if n == 0 or rc[k + 1] == 0:
+                    continue
+                c = f(f(f(n) * half_area(llo, lhi)) + f(f(rc[k + 1]) * ra[k + 1]))
+                if c < best[0]:
+                    best = (c, a, k + 1)
+        _, axis, split = best
+        if axis < 0:
+            continue
+        left = np.array([sah_bin(cen[i, axis], clo[axis], scale[axis]) < split for i in ids])
+        nl = int(left.sum())
+        if nl == 0 or nl == count:
+            continue
+        order[first:first + count] = np.concatenate([ids[left], ids[~left]])
+        L, R = used, used + 1
+        used += 2
+        bl, bh, _ = bins[axis]
+        lf[L], cnt[L], lf[R], cnt[R] = first, nl, first + nl, count - nl
+        nb[L] = np.concatenate([bl[:split].min(0), bh[:split].max(0)])
+        nb[R] = np.concatenate([bl[split:].min(0), bh[split:].max(0)])
+        lf[node], cnt[node] = L, 0
+        todo += [L, R]
+    return nb, lf, cnt, order, used
+
+
+@pytest.mark.parametrize("n_surfaces,seed", [(3, 4), (8, 2)])
+def test_binned_bvh_matches_restatement(nrt_mod, oracle_mod, n_surfaces, seed):
+    """The host binned builder equals the numpy restatement node for node and
+    slot for slot (the device builder is compared with the host builder on
+    the GPU, byte for byte)."""
+    from nrt import scenes
+
+    sc = scenes.surfaces_grid_scene(n_surfaces, seed=seed, width=8, height=8, spp=1)
+    P = oracle_mod.decompose_scene(sc.surfaces, f64=False)
+    boxes = nrt_mod.patch_bounds(P.cp, P.off, P.deg)
+    got = nrt_mod.build_bvh_binary(boxes, nrt_mod.BVH_BINNED_SAH)
+    ref = _binned_sah_restated(boxes)
+    assert got[4] == ref[4]
+    used = got[4]
+    assert np.array_equal(got[3], ref[3])
+    assert np.array_equal(got[1][:used], ref[1][:used]) and np.array_equal(got[2][:used], ref[2][:used])
+    assert np.array_equal(got[0][:used], ref[0][:used])
