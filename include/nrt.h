@@ -112,7 +112,7 @@ typedef struct {
     int max_leaf;       /* patches per BVH leaf (1..8, default 1) */
     int device;         /* CUDA device ordinal */
     int64_t wavefront_chunk; /* rays per wavefront pass (0 = 2^23); bounds its scratch,
-                                about 530 bytes per ray, allocated on first use */
+                                about 540 bytes per ray, allocated on first use */
 } nrt_build_opts;
 
 int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nrt_build_opts* opts,
@@ -235,7 +235,7 @@ typedef struct {
     int32_t class_blocks;    /* blocks of 256 threads per degree-class Newton launch */
     int32_t graph;           /* 1: rounds run inside one CUDA graph with a device-side loop (no host
                                 synchronisation); 2: host-driven rounds (one synchronisation each) */
-    int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 530 bytes per ray) */
+    int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 540 bytes per ray) */
     int32_t quota0;          /* candidates a ray emits in the first round, doubling per round ... */
     int32_t quota_max;       /* ... up to this many (<= 8); the default 4, then 8 */
 } nrt_wavefront_tuning;

@@ -521,10 +521,12 @@ __device__ __forceinline__ bool obb_misses(const float4* __restrict__ obb, const
 // makes a converged FP32 hit worse.  A step below 1e-7 in (u, v) ends the
 // refinement with a first-order move of S (no further evaluation): that is
 // the common case, one FP64 evaluation per hit.  S, dS/du, dS/dv and t are
-// those of the final (u, v), in double.
+// those of the final (u, v), in double.  Not inlined: every caller (Newton on
+// convergence, the wavefront's resolve from a recorded (u, v)) runs the same
+// machine code, so the result depends on nothing but (u, v) and the ray.
 template <int P, int Q>
-__device__ __forceinline__ void final_step_fp64(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
-                                                NewtonOut& o) {
+__device__ __noinline__ void final_step_fp64(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                             NewtonOut& o) {
     const double dx = r.dx, dy = r.dy, dz = r.dz;
     const double ax = fabs(dx), ay = fabs(dy), az = fabs(dz);
     double n1[3], n2[3];

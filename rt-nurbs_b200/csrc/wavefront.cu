@@ -21,7 +21,8 @@
 //                    on them, compacts the survivors by ballot into a shared
 //                    queue and runs Newton on full warps of survivors; a
 //                    converged hit with t > 0 lowers the ray's 64-bit key
-//                    (t bits << 32 | slot) with atomicMin.
+//                    (t bits << 32 | slot << 1 | flat) with a 128-bit
+//                    compare-and-swap that stores the hit's (u, v) beside it.
 //
 // The resolve pass sorts the rays that hit by their winner's (p, q, slot) and
 // k_wf_resolve<P,Q,LEARNED> recomputes each winning solve (same code and inputs) with
@@ -87,7 +88,7 @@ __device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long
         st[0] = 0;
         stt[0] = 0.f;
         best = INFINITY;
-        wb.best_key[i] = kNoHit;
+        wb.best[i] = make_ulonglong2(kNoHit, 0ull);
         if (tests) tests[i] = 0;
     } else {
         sp = wb.stack_sp[i];
@@ -95,7 +96,7 @@ __device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long
             st[k] = wb.stack_ref[(long long)k * n + i];
             stt[k] = wb.stack_t[(long long)k * n + i];
         }
-        best = key_t(wb.best_key[i]);
+        best = key_t(wb.best[i].x);
     }
     int32_t* emit = wb.emit_slot + (long long)j * kEmitMax;
     int emitted = 0;
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve_emit(long long n, Opts op, W
                                                          const int32_t* rank_of, unsigned long long* ctr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const unsigned long long key = wb.best_key[i];
+    const unsigned long long key = wb.best[i].x;
     if (key == kNoHit) {
         wb.emit_cnt[i] = 0;
         out.patch[i] = -1;
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve_emit(long long n, Opts op, W
             for (int a = 0; a < 9; ++a) out.geom[9 * (long long)i + a] = 0.f;
         return;
     }
-    const int s = (int)(key & 0xffffffffu);
+    const int s = (int)((key & 0xffffffffu) >> 1);
     wb.emit_cnt[i] = 1;
     wb.emit_slot[(long long)i * kEmitMax] = s;
     aggregated_add(wb.hist, rank_of[s]);
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve_emit(long long n, Opts op, W
 size_t wavefront_scratch_bytes(long long n, int n_slots) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t N = (size_t)n, S = (size_t)n_slots + 1;
-    return 2 * al(N * kStack * 4) + al(N * 4) + al(N * 8) + 2 * al(N * 4) + al(32) + al(N * kEmitMax * 4) +
+    return 2 * al(N * kStack * 4) + al(N * 4) + al(N * 16) + 2 * al(N * 4) + al(32) + al(N * kEmitMax * 4) +
            al(N * 4) + al(N * kEmitMax * sizeof(WfItem)) + 3 * al(S * 4) + al(64 * 4);
 }
 
@@ -355,7 +356,7 @@ WfBuffers wavefront_carve(void* base, long long n, int n_slots) {
     b.stack_ref = reinterpret_cast<int32_t*>(p); p += al(N * kStack * 4);
     b.stack_t = reinterpret_cast<float*>(p); p += al(N * kStack * 4);
     b.stack_sp = reinterpret_cast<int32_t*>(p); p += al(N * 4);
-    b.best_key = reinterpret_cast<unsigned long long*>(p); p += al(N * 8);
+    b.best = reinterpret_cast<ulonglong2*>(p); p += al(N * 16);
     b.active[0] = reinterpret_cast<int32_t*>(p); p += al(N * 4);
     b.active[1] = reinterpret_cast<int32_t*>(p); p += al(N * 4);
     b.counts = reinterpret_cast<int32_t*>(p); p += al(32);

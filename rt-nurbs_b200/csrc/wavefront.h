@@ -33,7 +33,8 @@ struct WfBuffers {
     int32_t* stack_ref;            // kStack * n, entry k of ray i at [k * n + i]
     float* stack_t;                // kStack * n
     int32_t* stack_sp;             // n
-    unsigned long long* best_key;  // n: (t bits << 32) | slot of the nearest hit so far
+    ulonglong2* best;              // n: the nearest hit so far, {key, (u bits << 32) | v bits}; the key
+                                   // (t bits << 32) | slot << 1 | flat orders hits by t, then slot
     int32_t* active[2];            // n each: ray indices still traversing (ping-pong)
     int32_t* counts;               // 8 ints: active counts of the two lists, round (graph), -, work
                                    // counters of the persistent step and scatter kernels (graph)

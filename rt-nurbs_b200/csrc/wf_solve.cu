@@ -67,6 +67,23 @@ __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const
     return newton<P, Q>(blk, r, pr, gu, gv, seed, nw);
 }
 
+// Lower the ray's nearest-hit record to {key, uv} if key is smaller: a 128-bit
+// compare-and-swap loop.  Every failed swap means another lane lowered the
+// key, so the loop ends after at most as many tries as there are competing
+// hits; the bound only guards against a fault, and reports false.
+__device__ __forceinline__ bool record_hit(ulonglong2* rec, unsigned long long key, unsigned long long uv) {
+    unsigned __int128* p = reinterpret_cast<unsigned __int128*>(rec);
+    const unsigned __int128 want = ((unsigned __int128)uv << 64) | key;
+    unsigned __int128 cur = *p;  // a torn read only costs one failed swap
+    for (int tries = 0; tries < (1 << 16); ++tries) {
+        if (key >= (unsigned long long)cur) return true;
+        const unsigned __int128 old = atomicCAS(p, cur, want);
+        if (old == cur) return true;
+        cur = old;
+    }
+    return false;
+}
+
 // Features of the lane's item for the network (zeros for an idle lane).
 __device__ __forceinline__ void item_features(const Scene& sc, bool valid, int slot, const int4& h, const double4& C,
                                               const RayFrame& r, const PatchRay& pr, float (&x)[kMlpIn]) {
@@ -96,7 +113,7 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
     int* qu = queue[warp];
     const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
     unsigned long long solves = 0, evals = 0, f64 = 0, culled = 0, hull_tests = 0, learned = 0, fallbacks = 0,
-                       flats = 0;
+                       flats = 0, cas_err = 0;
     NewtonOpts nw = op.nw;
     nw.fp64_final = 0;  // applied to the winner only, in k_wf_resolve
     const float cull_eps = op.nw.eps;
@@ -176,8 +193,11 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
             if (tests) atomicAdd(tests + it.ray, 1);
             flats += (unsigned long long)o.flat;
             if ((o.evals > 0 || o.flat) && o.t > 0.f) {
-                const unsigned long long key = ((unsigned long long)__float_as_uint(o.t) << 32) | (unsigned)it.slot;
-                atomicMin(wb.best_key + it.ray, key);
+                const unsigned long long key = ((unsigned long long)__float_as_uint(o.t) << 32) |
+                                               ((unsigned)it.slot << 1) | (unsigned)o.flat;
+                const unsigned long long uv =
+                    ((unsigned long long)__float_as_uint(o.u) << 32) | __float_as_uint(o.v);
+                if (!record_hit(wb.best + it.ray, key, uv)) ++cas_err;
             }
             if constexpr (MODE == kWfCollect) {  // a training pair: features -> converged (u, v), or (-1, -1)
                 const unsigned long long at = atomicAdd(op.col_count, 1ull);
@@ -202,13 +222,16 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
         if (evals) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, evals);
         if (hull_tests) atomicAdd(ctr + kHullByDegree + P * 8 + Q, hull_tests);
     }
+    if (ctr && cas_err) atomicAdd(ctr + kErrors, cas_err);
 }
 
 // Resolve, step 1: rays without a hit get their miss record; rays with one
 
-// Resolve, step 2 (one launch per degree class): recompute the winning solve
-// (same code and inputs, so the same iterate) with the FP64 final step, and
-// write the hit record.
+// Resolve, step 2 (one launch per degree class): rebuild the winning solve's
+// point from the (u, v) recorded with its key (one evaluation, the same one
+// the solve converged on), apply the FP64 final step, and write the hit
+// record; when per-ray evaluation counts are requested the solve itself is
+// run again instead (same code and inputs, so the same iterate).
 template <int P, int Q, bool LEARNED>
 __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int rank_lo, int rank_hi, Opts op,
                                                     Hits out, unsigned long long* ctr) {
@@ -244,10 +267,31 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
             mlp_infer_warp(*ms, warp, lane, x, lu, lv);
         }
         if (valid) {  // idle lanes wait at the __syncwarp below, so the next mma runs converged
-        int fell = 0;
-        const NewtonOut o = solve_item<P, Q, LEARNED>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
-                                                      (uint32_t)it.ray + op.seed_offset, op, op.nw, fell);
         const long long i = it.ray;
+        NewtonOut o;
+        if (out.iters) {  // the evaluation count is wanted: solve again
+            int fell = 0;
+            o = solve_item<P, Q, LEARNED>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv, (uint32_t)it.ray + op.seed_offset,
+                                          op, op.nw, fell);
+        } else {  // rebuild the winner at its recorded (u, v): the solve's last evaluation
+            const ulonglong2 rec = wb.best[i];
+            const float u = __uint_as_float((unsigned)(rec.y >> 32)), v = __uint_as_float((unsigned)rec.y);
+            const float* __restrict__ blk = sc.cp + h.x;
+            float H[4], Hu[4], Hv[4];
+            eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
+            const float iw = __frcp_rn(H[3]);
+            const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
+            o.fp64_solves = 0;
+            o.fp64_final = 0;
+            o.flat = (int)(rec.x & 1ull);
+            o.evals = o.flat ? 0 : 1;  // converged (the count itself is not recorded)
+            o.u = u; o.v = v;
+            o.sx = sx; o.sy = sy; o.sz = sz;
+            o.ux = (Hu[0] - sx * Hu[3]) * iw; o.uy = (Hu[1] - sy * Hu[3]) * iw; o.uz = (Hu[2] - sz * Hu[3]) * iw;
+            o.vx = (Hv[0] - sx * Hv[3]) * iw; o.vy = (Hv[1] - sy * Hv[3]) * iw; o.vz = (Hv[2] - sz * Hv[3]) * iw;
+            o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
+            if (!o.flat && op.nw.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+        }
         if ((o.evals > 0 || o.flat) && o.t > 0.f) {
             ++hits;
             f64f += (unsigned long long)o.fp64_final;
