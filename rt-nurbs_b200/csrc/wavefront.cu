@@ -481,6 +481,29 @@ cudaError_t capture(cudaStream_t cs, cudaGraph_t* g, F&& fill) {
     return le != cudaSuccess ? le : e;
 }
 
+// The degree classes' kernels of one step as parallel branches of the graph
+// being captured on cs: they touch disjoint work items and meet only in
+// atomics (the nearest-hit records, the counters), so the GPU may run one
+// class's blocks in another's tail.  launch(c) issues class c on L.stream.
+constexpr int kClassBranches = 4;
+
+template <class F>
+void fork_classes(cudaStream_t cs, cudaStream_t* side, cudaEvent_t* ev, int n_classes, WfClassLaunch& L,
+                  F&& launch) {
+    cudaEventRecord(ev[0], cs);
+    const int nb = std::min(n_classes, kClassBranches);
+    for (int b = 0; b < nb; ++b) cudaStreamWaitEvent(side[b], ev[0], 0);
+    for (int c = 0; c < n_classes; ++c) {
+        L.stream = side[c % kClassBranches];
+        launch(c);
+    }
+    for (int b = 0; b < nb; ++b) {
+        cudaEventRecord(ev[1 + b], side[b]);
+        cudaStreamWaitEvent(cs, ev[1 + b], 0);
+    }
+    L.stream = cs;
+}
+
 }  // namespace
 
 cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n,
@@ -494,6 +517,10 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
     cudaStream_t cs = nullptr;
     cudaError_t e = cudaGraphCreate(&g, 0);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    cudaStream_t side[kClassBranches] = {};
+    cudaEvent_t ev[1 + kClassBranches] = {};
+    for (int b = 0; b < kClassBranches && e == cudaSuccess; ++b) e = cudaStreamCreateWithFlags(&side[b], cudaStreamNonBlocking);
+    for (int b = 0; b < 1 + kClassBranches && e == cudaSuccess; ++b) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
     cudaGraphNode_t prev = nullptr;
     const int mode = op.init_mode == 2 ? kWfLearned : (op.col_feat ? kWfCollect : kWfPlain);
     for (long long at = 0; at < n && e == cudaSuccess; at += chunk) {
@@ -535,13 +562,13 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
                                                          tu.quota_max);
                 k_wf_scan<<<1, 1024, 0, cs>>>(plan.n_slots, wb);
                 k_wf_scatter_dev<<<scat_grid, 256, 0, cs>>>(rc, m, wb, plan.rank_of);
-                for (int c = 0; c < plan.n_classes; ++c) {
+                fork_classes(cs, side, ev, plan.n_classes, L, [&](int c) {
                     L.cls = c;
                     L.rank_lo = plan.class_rank[c];
                     L.rank_hi = plan.class_rank[c + 1];
                     L.grid = tu.class_blocks > 0 ? (unsigned)tu.class_blocks : plan.class_grid[c];
                     wf_newton_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
-                }
+                });
                 k_wf_round_end<<<1, 32, 0, cs>>>(wb, loop, ctr);
                 const cudaError_t le = cudaGetLastError();
                 cudaGraph_t got = nullptr;
@@ -557,13 +584,13 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
                 k_wf_resolve_emit<<<(unsigned)((m + 255) / 256), 256, 0, cs>>>(m, oc, wb, hc, plan.rank_of, ctr);
                 k_wf_scan<<<1, 1024, 0, cs>>>(plan.n_slots, wb);
                 k_wf_scatter<<<(unsigned)((m + 255) / 256), 256, 0, cs>>>(rc, 0, (int)m, wb, 0, plan.rank_of);
-                for (int c = 0; c < plan.n_classes; ++c) {
+                fork_classes(cs, side, ev, plan.n_classes, L, [&](int c) {
                     L.cls = c;
                     L.rank_lo = plan.class_rank[c];
                     L.rank_hi = plan.class_rank[c + 1];
                     L.grid = plan.class_grid[c];
                     wf_resolve_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
-                }
+                });
             });
         cudaGraphNode_t n_post = nullptr;
         if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_post, g, &n_loop, 1, post);
@@ -575,6 +602,10 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
     if (e != cudaSuccess) *exec = nullptr;
     if (g) cudaGraphDestroy(g);
     if (cs) cudaStreamDestroy(cs);
+    for (cudaStream_t st : side)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
     return e;
 }
 
