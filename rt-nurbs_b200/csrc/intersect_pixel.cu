@@ -23,7 +23,7 @@ struct Tally {
     unsigned long long box, cand, culled, solves, evals, f64s, f64f, err, flat;
 };
 
-template <int P, int Q>
+template <int P, int Q, bool FINAL>
 __device__ __forceinline__ void test_patch(const Scene& sc, int slot, const RayFrame& r, float te, const Opts& op,
                                            uint32_t seed, Best& b, Tally& c, unsigned long long* ctr) {
     const int4 h = sc.hdr[slot];
@@ -49,7 +49,7 @@ __device__ __forceinline__ void test_patch(const Scene& sc, int slot, const RayF
             return;
         }
     }
-    const NewtonOut o = newton<P, Q>(blk, r, pr, gu, gv, seed, op.nw);
+    const NewtonOut o = newton<P, Q, FINAL>(blk, r, pr, gu, gv, seed, op.nw);
     ++c.solves;
     c.evals += (unsigned long long)(o.evals > 0 ? o.evals : -o.evals);
     c.f64s += (unsigned long long)o.fp64_solves;
@@ -63,18 +63,20 @@ __device__ __forceinline__ void test_patch(const Scene& sc, int slot, const RayF
 }
 
 // Degree dispatch: one specialised, fully unrolled instantiation per (p, q).
+template <bool FINAL>
 __device__ __noinline__ void test_patch_any(const Scene& sc, int slot, const RayFrame& r, float te, const Opts& op,
                                             uint32_t seed, Best& b, Tally& c, unsigned long long* ctr) {
     const int pq = sc.hdr[slot].y & 0xff;
     switch (pq) {
 #define NRT_CASE(P, Q) \
-    case (P) | ((Q) << 4): test_patch<P, Q>(sc, slot, r, te, op, seed, b, c, ctr); break;
+    case (P) | ((Q) << 4): test_patch<P, Q, FINAL>(sc, slot, r, te, op, seed, b, c, ctr); break;
         NRT_FOR_EACH_DEGREE(NRT_CASE)
 #undef NRT_CASE
         default: ++c.err; break;
     }
 }
 
+template <bool FINAL>
 __device__ __forceinline__ void trace_pixel(const Scene& sc, const Rays& rays, long long i, const Opts& op,
                                             const Hits& out, unsigned long long* ctr) {
     RayFrame r;
@@ -139,7 +141,7 @@ __device__ __forceinline__ void trace_pixel(const Scene& sc, const Rays& rays, l
             }
         } else {
             const int first = leaf_first(ref), cnt = leaf_count(ref);
-            for (int s = first; s < first + cnt; ++s) test_patch_any(sc, s, r, te, op, seed, b, c, ctr);
+            for (int s = first; s < first + cnt; ++s) test_patch_any<FINAL>(sc, s, r, te, op, seed, b, c, ctr);
         }
     }
     if (b.slot >= 0) {
@@ -183,19 +185,23 @@ __device__ __forceinline__ void trace_pixel(const Scene& sc, const Rays& rays, l
     }
 }
 
+// FINAL: instantiated with and without the FP64 final step (op.nw.fp64_final
+// picks one at launch).
+template <bool FINAL>
 __global__ void __launch_bounds__(128) k_intersect_pixel(Scene sc, Rays rays, long long n, Opts op, Hits out,
                                                          unsigned long long* ctr) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) trace_pixel(sc, rays, i, op, out, ctr);
+    if (i < n) trace_pixel<FINAL>(sc, rays, i, op, out, ctr);
 }
 
 // Same, for the ray indices list[0 .. *count) (count known only on the device).
+template <bool FINAL>
 __global__ void __launch_bounds__(128) k_intersect_pixel_list(Scene sc, Rays rays, const int32_t* list,
                                                               const int32_t* count, Opts op, Hits out,
                                                               unsigned long long* ctr) {
     const int m = *count;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
-        trace_pixel(sc, rays, list[k], op, out, ctr);
+        trace_pixel<FINAL>(sc, rays, list[k], op, out, ctr);
 }
 
 cudaError_t launch_intersect_pixel(const Scene& sc, const Rays& rays, long long n, const Opts& op, const Hits& out,
@@ -203,7 +209,8 @@ cudaError_t launch_intersect_pixel(const Scene& sc, const Rays& rays, long long 
     if (n <= 0) return cudaSuccess;
     const int threads = 128;
     const long long blocks = (n + threads - 1) / threads;
-    k_intersect_pixel<<<(unsigned)blocks, threads, 0, stream>>>(sc, rays, n, op, out, ctr);
+    if (op.nw.fp64_final) k_intersect_pixel<true><<<(unsigned)blocks, threads, 0, stream>>>(sc, rays, n, op, out, ctr);
+    else k_intersect_pixel<false><<<(unsigned)blocks, threads, 0, stream>>>(sc, rays, n, op, out, ctr);
     return cudaGetLastError();
 }
 
@@ -213,7 +220,10 @@ cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const
     if (max_n <= 0) return cudaSuccess;
     long long blocks = (max_n + 127) / 128;
     if (blocks > 148 * 8) blocks = 148 * 8;
-    k_intersect_pixel_list<<<(unsigned)blocks, 128, 0, stream>>>(sc, rays, list, list_count, op, out, ctr);
+    if (op.nw.fp64_final)
+        k_intersect_pixel_list<true><<<(unsigned)blocks, 128, 0, stream>>>(sc, rays, list, list_count, op, out, ctr);
+    else
+        k_intersect_pixel_list<false><<<(unsigned)blocks, 128, 0, stream>>>(sc, rays, list, list_count, op, out, ctr);
     return cudaGetLastError();
 }
 

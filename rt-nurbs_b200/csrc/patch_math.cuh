@@ -617,7 +617,9 @@ __device__ __noinline__ void final_step_fp64(const float* __restrict__ blk, cons
 // BezierPatchOps::newtonRhapson (src/math/bezier_patch.h:197-266).  When
 // cond_fp64 > 0 and ||J||_F^2 / |det J| exceeds it, the 2x2 solve is done in
 // FP64 (products of floats are exact there, so det J has no cancellation).
-template <int P, int Q>
+// FINAL = false compiles the FP64 final step out (for kernels that run
+// without it, so that they carry no call to it).
+template <int P, int Q, bool FINAL = true>
 __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
                                             float u0, float v0, uint32_t seed, const NewtonOpts& op) {
     NewtonOut o;
@@ -641,23 +643,19 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
             o.ux = ux; o.uy = uy; o.uz = uz;
             o.vx = vx; o.vy = vy; o.vz = vz;
             o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
-            if (op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+            if (FINAL && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
             return o;
         }
         const float j11 = r.n1x * ux + r.n1y * uy + r.n1z * uz;
         const float j21 = r.n2x * ux + r.n2y * uy + r.n2z * uz;
         const float j12 = r.n1x * vx + r.n1y * vy + r.n1z * vz;
         const float j22 = r.n2x * vx + r.n2y * vy + r.n2z * vz;
+        seed = pcg_hash(seed);
+        const float rnd1 = (float)seed * 2.3283064e-10f;
+        seed = pcg_hash(seed);
+        const float rnd2 = (float)seed * 2.3283064e-10f;
         const float det = j11 * j22 - j12 * j21;
         if (fabsf(det) < op.det_eps) {
-            // the reference advances the seed twice every iteration; the pull of
-            // iteration `it` uses its (2 it - 1)-th and (2 it)-th hashes, formed
-            // here only when they are needed
-            uint32_t s = seed;
-            for (int k = 1; k < 2 * it; ++k) s = pcg_hash(s);
-            const float rnd1 = (float)s * 2.3283064e-10f;
-            s = pcg_hash(s);
-            const float rnd2 = (float)s * 2.3283064e-10f;
             u = u + 0.1f * ((u0 - u) * rnd1);
             v = v + 0.1f * ((v0 - v) * rnd2);
         } else if (op.cond_fp64 > 0.f &&
