@@ -144,16 +144,15 @@ def ncu_traffic(kernel_tag):
 def cpu_reference_rate(scene_def, rays_np, seconds=10.0, iters=8, eps=1e-6, port=False):
     """Mrays/s of the reference's own FP32 path on the host cores (oracle/_ref,
     OpenMP over rays) on a bounded sample of the workload's rays.  The BVH is
-    this project's binned-SAH tree exported in the reference's node layout (the
-    reference's own O(N^2) builder takes minutes at this size; the closest hit
-    does not depend on the tree)."""
-    import nrt
+    the 32-bin SAH tree in the reference's node layout, built by the oracle's
+    own C restatement (the reference's O(N^2) builder takes minutes at this
+    size; the closest hit does not depend on the tree), so this arm loads
+    nothing of the engine."""
     import oracle
 
     P = oracle.decompose_scene(scene_def.surfaces, f64=False)
-    boxes = nrt.patch_bounds(P.cp, P.off, P.deg)
-    nb, lf, cnt, order, used = nrt.build_bvh_binary(boxes, nrt.BVH_BINNED_SAH)
-    bvh = oracle.BinaryBVH(nb, lf, cnt, order, used)
+    bvh = oracle.build_bvh_binned(oracle.patch_boxes(P))
+    order = bvh.order
     use_ref = oracle.ref_available(iters) and not port
     Pb = P.subset(order)
     n = rays_np.n
@@ -238,7 +237,8 @@ def reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "sample_rays_per_step": int(cb["idx"].size)},
+            "config": {"workload": WORKLOAD, "sample_rays_per_step": int(cb["idx"].size),
+                       "sample": cb["sample"] + "; Mrays/s = sample rays / CPU seconds, the rate of the whole workload"},
             "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cb["cores"], "kind": cb["kind"],
                              "sample": cb["sample"]},
             "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

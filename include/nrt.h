@@ -218,9 +218,15 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
  * library holds until the process exits; rays go through in passes that fit
  * that array.  Scenes too large for it (about 5 million patches and more) are
  * rejected with NRT_ERR_INVALID.  The first call on a device looks the array
- * up (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the one array, so calls whose work overlaps on the GPU race:
- * serialise them on one stream.  Synchronises `stream` once per round. */
+ * up (cudaGetSymbolAddress) and keeps its address for the life of the process;
+ * after a cudaDeviceReset (or any other teardown of the device's primary
+ * context) that address is stale and this entry point must not be called
+ * again in the process.  The call synchronises `stream` once per round to read
+ * the number of rays still traversing into a host word, so it must not be
+ * called while `stream`, or any other stream of that device, is being captured
+ * into a CUDA graph.  All calls share the one array, so calls whose work
+ * overlaps on the GPU race: serialise them on one stream.  Rounds run with the
+ * scene's round quotas (nrt_scene_set_tuning), as nrt_intersect does. */
 int nrt_intersect_noalloc(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_intersect_opts* opts,
                           const nrt_hits* hits, void* stream);
 

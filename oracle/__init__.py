@@ -40,11 +40,18 @@ class OrcOpts(C.Structure):
                 ("flat_threshold", C.c_float), ("cam_k", C.c_float)]
 
 
+def reference_dir() -> str:
+    """The reference checkout whose sources `make ref` compiles: $NRT_REFERENCE,
+    else the build container's mount point (absent on the GPU hosts, where the
+    prebuilt _ref libraries are used)."""
+    return os.environ.get("NRT_REFERENCE", "/root/reference")
+
+
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and, if ref and the reference sources exist, the _ref libraries)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if ref and os.path.isdir(os.path.join(reference_dir(), "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"NRT_REFERENCE={reference_dir()}"], check=True)
 
 
 def lib():
@@ -61,6 +68,8 @@ def lib():
         L.orc_patch_boxes.argtypes = [f32p, i32p, i32p, C.c_int, f32p]
         L.orc_build_bvh.argtypes = [f32p, C.c_int, f32p, u32p, u32p, i32p]
         L.orc_build_bvh.restype = C.c_int
+        L.orc_build_bvh_binned.argtypes = [f32p, C.c_int, C.c_int, f32p, u32p, u32p, i32p]
+        L.orc_build_bvh_binned.restype = C.c_int
         common = [i32p, i32p, C.c_void_p, f32p, u32p, u32p, i32p, f32p, f32p, f32p, f32p, f32p, f32p, C.c_long,
                   C.POINTER(OrcOpts), i32p]
         L.orc_intersect_f32.argtypes = [f32p] + common + [f32p, f32p, f32p, i32p, i32p, C.c_void_p,
@@ -190,6 +199,19 @@ def build_bvh(boxes: np.ndarray) -> BinaryBVH:
     cnt = np.zeros(M, np.uint32)
     order = np.zeros(N, np.int32)
     used = lib().orc_build_bvh(np.ascontiguousarray(boxes, np.float32), N, nb, lf, cnt, order)
+    return BinaryBVH(nb, lf, cnt, order, used)
+
+
+def build_bvh_binned(boxes: np.ndarray, max_leaf: int = 1) -> BinaryBVH:
+    """32-bin SAH binary BVH (the tree this project builds for scenes), from
+    the oracle's own C restatement."""
+    N = boxes.shape[0]
+    M = max(2 * N - 1, 1)
+    nb = np.zeros((M, 6), np.float32)
+    lf = np.zeros(M, np.uint32)
+    cnt = np.zeros(M, np.uint32)
+    order = np.zeros(N, np.int32)
+    used = lib().orc_build_bvh_binned(np.ascontiguousarray(boxes, np.float32), N, max_leaf, nb, lf, cnt, order)
     return BinaryBVH(nb, lf, cnt, order, used)
 
 

@@ -935,11 +935,12 @@ int noalloc_views(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     if (!(o.eps > 0.f)) return fail(NRT_ERR_INVALID, "eps must be positive");
     if (o.init_mode != NRT_INIT_MIDPOINT && o.init_mode != NRT_INIT_BILINEAR)
         return fail(NRT_ERR_UNSUPPORTED, "init mode %d not available without allocation", o.init_mode);
-    if (o.flat_threshold > 0.f) return fail(NRT_ERR_UNSUPPORTED, "flat-skip runs on the per-pixel schedule only");
     v->scene = scene->view;
     v->plan = scene->plan;
     v->counters = scene->counters;
     v->device = scene->device;
+    v->quota0 = scene->tuning.quota0;  // the round quotas nrt_intersect runs with
+    v->quota_max = scene->tuning.quota_max;
     to_dev_opts(o, v->opts, scene->counters_on);
     return NRT_OK;
 }

@@ -21,8 +21,8 @@ struct __align__(16) WfItem {
 constexpr unsigned long long kNoHit = ~0ull;
 
 // Candidates per ray in round r: q0, 2 q0, 4 q0, ... up to qmax (the
-// launch-shape default is 4, then 8; the noalloc and collection paths use
-// 1, 2, 4, 8).  qmax <= 8 keeps a round's emissions (quota plus the rest
+// launch-shape default is 4, then 8, and nrt_intersect_noalloc runs with the
+// scene's tuned values too; the training-pair collection uses 1, 2, 4, 8).  qmax <= 8 keeps a round's emissions (quota plus the rest
 // of one leaf of <= 8 patches) within kEmitMax.
 __host__ __device__ constexpr int round_quota(int r, int q0 = 1, int qmax = 8) {
     return r >= 4 ? qmax : ((q0 << r) < qmax ? (q0 << r) : qmax);
@@ -143,6 +143,7 @@ struct NoallocViews {
     dev::Opts opts;
     unsigned long long* counters;
     int device;
+    int quota0, quota_max;
 };
 
 }  // namespace nrt

@@ -149,8 +149,13 @@ def main():
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     mlp.save(args.out)
     res = evaluate(mlp, learned_iters=args.learned_iters)
-    print(json.dumps({"pairs": int(feats.shape[0]), "epochs": args.epochs, "train_s": round(secs, 2),
-                      "loss": [float(x) for x in losses], "eval_unseen_mixed64_seed1": res}))
+    meta = {"model": os.path.basename(args.out), "pairs": int(feats.shape[0]), "epochs": args.epochs,
+            "batch": args.batch, "lr": args.lr, "train_s": round(secs, 2), "loss": [float(x) for x in losses],
+            "eval_unseen_mixed64_seed1": res}
+    # the model's metadata beside it: how it was trained and what it gained on an unseen scene
+    with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
+        json.dump(meta, f, indent=1)
+    print(json.dumps(meta))
 
 
 if __name__ == "__main__":

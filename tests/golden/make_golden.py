@@ -8,7 +8,7 @@ as .npz files.  The tests then pin this project's oracle restatement against
 these files without needing the reference at test time.
 
 Usage (needs the reference sources at build time of oracle/_ref):
-    make -C oracle ref && python tests/golden/make_golden.py
+    NRT_REFERENCE=<reference checkout> make -C oracle ref && python tests/golden/make_golden.py
 """
 import os
 import sys

@@ -221,7 +221,8 @@ def _binned_sah_restated(boxes, max_leaf=1):
 def test_binned_bvh_matches_restatement(nrt_mod, oracle_mod, n_surfaces, seed):
     """The host binned builder equals the numpy restatement node for node and
     slot for slot (the device builder is compared with the host builder on
-    the GPU, byte for byte)."""
+    the GPU, byte for byte), and so does the oracle's C builder that the
+    reference arm of the bench uses."""
     from nrt import scenes
 
     sc = scenes.surfaces_grid_scene(n_surfaces, seed=seed, width=8, height=8, spp=1)
@@ -234,3 +235,7 @@ def test_binned_bvh_matches_restatement(nrt_mod, oracle_mod, n_surfaces, seed):
     assert np.array_equal(got[3], ref[3])
     assert np.array_equal(got[1][:used], ref[1][:used]) and np.array_equal(got[2][:used], ref[2][:used])
     assert np.array_equal(got[0][:used], ref[0][:used])
+    orc = oracle_mod.build_bvh_binned(oracle_mod.patch_boxes(P))
+    assert orc.used == used and np.array_equal(orc.order, ref[3])
+    assert np.array_equal(orc.lf[:used], ref[1][:used]) and np.array_equal(orc.cnt[:used], ref[2][:used])
+    assert np.array_equal(orc.box[:used], ref[0][:used])

@@ -6,7 +6,9 @@ with the tolerance of the other wavefront tests (identical hit/miss on
 >= 99.99% of rays, same patch on >= 99.9% of rays both hit, bit-equal t, u, v
 where the patch is the same), on two calls in a row (the second one runs on the
 array the first left behind).  The ray batch is larger than one pass through
-the array, so the passes are exercised too.
+the array, so the passes are exercised too.  The property the entry point
+exists for is checked as well: after a warm-up call, a further call leaves the
+device's free memory (cudaMemGetInfo) exactly where it was.
 """
 import ctypes as C
 
@@ -60,16 +62,23 @@ def assert_same(a, b):
 
 
 def test_noalloc_matches_wavefront_twice(nrt_gpu):
+    import torch
+
     from nrt import scenes
 
     sc = scenes.surfaces_grid_scene(16, seed=5, width=400, height=240, spp=2)  # 192,000 rays
     scene = nrt_gpu.Scene(sc.surfaces)
     rays = nrt_gpu.camera_rays(sc.camera)
+    cam_k = float(sc.camera.cam_k)
     for opts in [nrt_gpu.default_opts(fp64_final=1, cond_fp64=1e4, schedule=nrt_gpu.SCHED_WAVEFRONT),
-                 nrt_gpu.reference_opts(hull_cull=1, schedule=nrt_gpu.SCHED_WAVEFRONT)]:
+                 nrt_gpu.reference_opts(hull_cull=1, schedule=nrt_gpu.SCHED_WAVEFRONT),
+                 nrt_gpu.reference_opts(flat_threshold=2.0, cam_k=cam_k, schedule=nrt_gpu.SCHED_WAVEFRONT)]:
         ref = {k: v.cpu().numpy() for k, v in scene.intersect(rays, opts).items()}
         assert (ref["patch"] >= 0).mean() > 0.3
         first = call_noalloc(nrt_gpu, scene, rays, opts)
+        free_before = torch.cuda.mem_get_info()[0]
         second = call_noalloc(nrt_gpu, scene, rays, opts)
+        free_after = torch.cuda.mem_get_info()[0]
+        assert free_after == free_before, (free_before, free_after)
         assert_same(ref, first)
         assert_same(ref, second)
