@@ -70,6 +70,9 @@ def lib():
         L.orc_build_bvh.restype = C.c_int
         L.orc_build_bvh_binned.argtypes = [f32p, C.c_int, C.c_int, f32p, u32p, u32p, i32p]
         L.orc_build_bvh_binned.restype = C.c_int
+        L.orc_roots_f64.argtypes = [f64p, i32p, i32p, f32p, C.c_int] + [f32p] * 6 + [
+            C.c_long, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, i32p, f64p, f64p, f64p,
+            C.c_void_p]
         common = [i32p, i32p, C.c_void_p, f32p, u32p, u32p, i32p, f32p, f32p, f32p, f32p, f32p, f32p, C.c_long,
                   C.POINTER(OrcOpts), i32p]
         L.orc_intersect_f32.argtypes = [f32p] + common + [f32p, f32p, f32p, i32p, i32p, C.c_void_p,
@@ -284,6 +287,44 @@ def intersect(P: Patches, bvh: BinaryBVH, rays: Rays, init_mode: int = 0, max_it
        *rays.arrays(), R, C.byref(opts), hit, t, u, v, ev, te, None if g is None else g.ctypes.data, C.byref(nc),
        C.byref(sc))
     return Hits(hit, t, u, v, ev, te, g, nc.value, sc.value)
+
+
+@dataclass
+class Roots:
+    patch: np.ndarray   # nearest root's patch (input order), -1 = none
+    t: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    n_roots: np.ndarray | None
+
+
+def true_closest_hits(P: Patches, rays: Rays, grid: int = 4, max_iter: int = 40, eps: float = 1e-11) -> Roots:
+    """Multi-start FP64 diagnostic: for every ray the nearest root over all
+    patches whose box it crosses, from a grid x grid lattice of Newton starts
+    plus the midpoint on each (double, eps on |r1|+|r2|), with the number of
+    distinct roots found.  Needs P.cp64."""
+    R = rays.n
+    patch = np.zeros(R, np.int32)
+    t, u, v = (np.zeros(R, np.float64) for _ in range(3))
+    nr = np.zeros(R, np.int32)
+    lib().orc_roots_f64(P.cp64, P.off, P.deg, patch_boxes(P), P.n, *rays.arrays(), R, grid, max_iter, eps, None,
+                        None, None, patch, t, u, v, nr.ctypes.data)
+    return Roots(patch, t, u, v, nr)
+
+
+def polish_hits(P: Patches, rays: Rays, patch: np.ndarray, u0: np.ndarray, v0: np.ndarray, max_iter: int = 40,
+                eps: float = 1e-11) -> Roots:
+    """FP64 Newton on patch[i] from (u0[i], v0[i]) (patch < 0: skipped): the
+    exact root next to a reported hit, or patch -1 where none is reached."""
+    R = rays.n
+    only = np.ascontiguousarray(patch, np.int32)
+    a0 = np.ascontiguousarray(u0, np.float64)
+    b0 = np.ascontiguousarray(v0, np.float64)
+    out = np.zeros(R, np.int32)
+    t, u, v = (np.zeros(R, np.float64) for _ in range(3))
+    lib().orc_roots_f64(P.cp64, P.off, P.deg, patch_boxes(P), P.n, *rays.arrays(), R, 0, max_iter, eps,
+                        only.ctypes.data, a0.ctypes.data, b0.ctypes.data, out, t, u, v, None)
+    return Roots(out, t, u, v, None)
 
 
 def newton_f32(cp: np.ndarray, p: int, q: int, o, d, u0=0.5, v0=0.5, det_eps=1e-5, eps=1e-6, seed=0, max_iter=8):

@@ -709,6 +709,114 @@ void orc_intersect_f64(const double* cp, const int* cp_off, const int* deg, cons
                            skip_total);
 }
 
+// "True closest hit" diagnostic (FP64, multi-start).  Newton from the patch
+// midpoint (the method) finds at most one root of each patch it tests, and the
+// root it finds depends on the basin the start lies in; when the engine and
+// the FP64 oracle disagree, this tells "another root of the same surface" and
+// "a root the single start missed" apart from a wrong answer.  For every ray
+// and every patch whose box (widened by 1e-4 of its extent) the ray crosses,
+// plain Newton in double (no random pull: a singular step abandons the start)
+// runs from a grid x grid lattice of starts ((i + 1/2) / grid) and from
+// (1/2, 1/2), up to max_iter steps, converged when |r1| + |r2| < eps; the roots
+// with t > 0 are collected, coincident ones (|du| + |dv| < 1e-7 on one patch)
+// counted once.  Output per ray: the nearest root (patch in input order, -1
+// if none; t, u, v) and the number of distinct roots.  With only_patch set,
+// polish mode: one start (u0[i], v0[i]) on patch only_patch[i] (< 0: skipped),
+// no box test; patch_out[i] = only_patch[i] if it converged, else -1.
+static bool newton_polish(const Planes<double>& pl, const V4<double>* P, int p, int q, double& u, double& v,
+                          int max_iter, double eps, V3<double>& S_out) {
+    for (int it = 0; it < max_iter; ++it) {
+        V4<double> H, Hu, Hv;
+        patch_eval(P, p, q, u, v, H, Hu, Hv);
+        const double iw = 1.0 / H.w;
+        const V3<double> S = {H.x * iw, H.y * iw, H.z * iw};
+        const V3<double> Su = {(Hu.x - S.x * Hu.w) * iw, (Hu.y - S.y * Hu.w) * iw, (Hu.z - S.z * Hu.w) * iw};
+        const V3<double> Sv = {(Hv.x - S.x * Hv.w) * iw, (Hv.y - S.y * Hv.w) * iw, (Hv.z - S.z * Hv.w) * iw};
+        const double r0 = dot3(pl.n1, S) + pl.d1, r1 = dot3(pl.n2, S) + pl.d2;
+        if (std::fabs(r0) + std::fabs(r1) < eps) {
+            S_out = S;
+            return true;
+        }
+        const double j0 = dot3(pl.n1, Su), j1 = dot3(pl.n2, Su), j2 = dot3(pl.n1, Sv), j3 = dot3(pl.n2, Sv);
+        const double det = j0 * j3 - j2 * j1;
+        if (det == 0.0 || !std::isfinite(det)) return false;
+        u = std::fmin(std::fmax(u - (j3 * r0 - j2 * r1) / det, 0.0), 1.0);
+        v = std::fmin(std::fmax(v - (j0 * r1 - j1 * r0) / det, 0.0), 1.0);
+    }
+    return false;
+}
+
+void orc_roots_f64(const double* cp, const int* cp_off, const int* deg, const float* boxes, int N, const float* ox,
+                   const float* oy, const float* oz, const float* dx, const float* dy, const float* dz, long R,
+                   int grid, int max_iter, double eps, const int32_t* only_patch, const double* u0,
+                   const double* v0, int32_t* patch_out, double* t_out, double* u_out, double* v_out,
+                   int32_t* n_roots_out) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long i = 0; i < R; ++i) {
+        const V3<double> o = {ox[i], oy[i], oz[i]}, d = {dx[i], dy[i], dz[i]};
+        const Planes<double> pl = ray_planes<double>(o, d);
+        patch_out[i] = -1;
+        t_out[i] = -1.0;
+        u_out[i] = v_out[i] = 0.0;
+        if (n_roots_out) n_roots_out[i] = 0;
+        auto t_of = [&](const V3<double>& S) { return (S.x - o.x) * d.x + (S.y - o.y) * d.y + (S.z - o.z) * d.z; };
+        if (only_patch) {
+            const int k = only_patch[i];
+            if (k < 0) continue;
+            double u = u0[i], v = v0[i];
+            V3<double> S;
+            if (newton_polish(pl, reinterpret_cast<const V4<double>*>(cp) + cp_off[k], deg[2 * k], deg[2 * k + 1], u,
+                              v, max_iter, eps, S)) {
+                patch_out[i] = k;
+                t_out[i] = t_of(S);
+                u_out[i] = u;
+                v_out[i] = v;
+            }
+            continue;
+        }
+        const float of[3] = {ox[i], oy[i], oz[i]};
+        const float rd[3] = {1 / dx[i], 1 / dy[i], 1 / dz[i]};
+        double best = INFINITY;
+        int n_roots = 0;
+        std::vector<double> ru, rv;
+        for (int k = 0; k < N; ++k) {
+            float b[6];
+            for (int a = 0; a < 3; ++a) {
+                const float w = 1e-4f * (boxes[6 * k + 3 + a] - boxes[6 * k + a]) + 1e-6f;
+                b[a] = boxes[6 * k + a] - w;
+                b[3 + a] = boxes[6 * k + 3 + a] + w;
+            }
+            if (!(slab(b, of, rd) < INFINITY)) continue;
+            const V4<double>* P = reinterpret_cast<const V4<double>*>(cp) + cp_off[k];
+            const int p = deg[2 * k], q = deg[2 * k + 1];
+            ru.clear();
+            rv.clear();
+            for (int s = 0; s <= grid * grid; ++s) {
+                double u = s == grid * grid ? 0.5 : (s / grid + 0.5) / grid;
+                double v = s == grid * grid ? 0.5 : (s % grid + 0.5) / grid;
+                V3<double> S;
+                if (!newton_polish(pl, P, p, q, u, v, max_iter, eps, S)) continue;
+                const double t = t_of(S);
+                if (!(t > 0)) continue;
+                bool seen = false;
+                for (size_t r = 0; r < ru.size() && !seen; ++r) seen = std::fabs(ru[r] - u) + std::fabs(rv[r] - v) < 1e-7;
+                if (seen) continue;
+                ru.push_back(u);
+                rv.push_back(v);
+                ++n_roots;
+                if (t < best) {
+                    best = t;
+                    patch_out[i] = k;
+                    t_out[i] = t;
+                    u_out[i] = u;
+                    v_out[i] = v;
+                }
+            }
+        }
+        if (n_roots_out) n_roots_out[i] = n_roots;
+    }
+}
+
 // Single (ray, patch) Newton solve, for unit tests of the per-patch step.
 int orc_newton_f32(const float* cp, int p, int q, const float* o, const float* d, float u0, float v0, float det_eps,
                    float eps, uint32_t seed, int max_iter, float* out /* u, v, S(3), Su(3), Sv(3) */) {

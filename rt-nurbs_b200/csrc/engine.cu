@@ -191,7 +191,8 @@ void finish_scene(nrt_scene* sc, const ArenaLayout& L, int N, dev::WfPlan plan, 
     sc->n_surfaces = n_surfaces;
 }
 
-int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_scene** out) {
+int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_scene** out, const BinaryBVH* given,
+                const float* delta_by_patch) {
     if (!out) return fail(NRT_ERR_INVALID, "out is null");
     *out = nullptr;
     const int N = ps.count();
@@ -208,11 +209,12 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
         if (p < 1 || q < 1 || p > NRT_MAX_DEGREE || q > NRT_MAX_DEGREE)
             return fail(NRT_ERR_INVALID, "patch %d has degree (%d,%d) outside 1..%d", k, p, q, NRT_MAX_DEGREE);
     }
-    // BVH over patch boxes
+    // BVH over patch boxes (or the caller's tree)
     std::vector<Box3> boxes;
     patch_boxes(ps, boxes);
     BinaryBVH bin;
-    if (o.builder == NRT_BVH_EXACT_SAH) build_exact_sah(boxes, bin);
+    if (given) bin = *given;
+    else if (o.builder == NRT_BVH_EXACT_SAH) build_exact_sah(boxes, bin);
     else build_binned_sah(boxes, o.max_leaf, bin);
     for (int i = 0; i < bin.used; ++i)
         if (bin.prim_count[i] > 8)  // coincident centroids can leave bigger leaves
@@ -253,6 +255,7 @@ int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_s
         const int p = ps.deg[2 * k], q = ps.deg[2 * k + 1];
         pack_slot(&ps.cp[4 * (size_t)ps.off[k]], p, q, boxes[k], k, ps.surf[k], (long long)off, &blocks[off], hdr[s],
                   centre[s], &corners[4 * (size_t)s], delta[s], frames[s], &obbs[4 * (size_t)s]);
+        if (delta_by_patch) delta[s] = delta_by_patch[k];  // the caller's flatness values
         info.degree_hist[p * 8 + q] += 1;
         off += 4 * (size_t)dev::padded_points(p, q);
     }
@@ -306,6 +309,7 @@ void to_dev_opts(const nrt_intersect_opts& o, dev::Opts& d, int counters) {
     d.nw.det_eps = o.det_eps;
     d.nw.cond_fp64 = o.cond_fp64;
     d.nw.fp64_final = o.fp64_final;
+    d.nw.fp64_band = o.fp64_final ? 1 : 0;  // the FP64 final-step mode decides convergence near eps in FP64
     d.init_mode = o.init_mode;
     d.hull_cull = o.hull_cull;
     d.seed_offset = (uint32_t)o.seed_offset;

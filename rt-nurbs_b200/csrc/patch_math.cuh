@@ -47,7 +47,13 @@ struct NewtonOpts {
     float det_eps;
     float cond_fp64;
     int fp64_final;
+    int fp64_band;   // 1: convergence near eps is decided in FP64 (newton_tail_fp64)
 };
+
+// The FP64 decision band: an FP32 residual below kBandLo * eps is accepted as
+// converged; one in [kBandLo * eps, kBandHi * eps) hands the solve to FP64,
+// which decides whether (and where) it converges within the remaining budget.
+constexpr float kBandLo = 0.125f, kBandHi = 16.f;
 
 struct NewtonOut {
     int evals;       // > 0 converged after this many evaluations; < 0 not converged
@@ -612,13 +618,105 @@ __device__ __noinline__ void final_step_fp64(const float* __restrict__ blk, cons
     o.fp64_final = 1;
 }
 
+// The ray's two planes rebuilt in double from the (float) ray, as the FP64
+// oracle forms them (MathUtils::getRayPlanes, src/math/math_utils.h:33-54, in
+// double), with the offsets of the patch-local frame.
+struct PlanesF64 {
+    double n1[3], n2[3], e1, e2;
+};
+__device__ __forceinline__ PlanesF64 planes_fp64(const RayFrame& r, const PatchRay& pr) {
+    const double dx = r.dx, dy = r.dy, dz = r.dz;
+    const double ax = fabs(dx), ay = fabs(dy), az = fabs(dz);
+    PlanesF64 p;
+    if (ax > ay && ax > az) {
+        const double l = sqrt(dx * dx + dy * dy);
+        p.n1[0] = dy / l; p.n1[1] = -dx / l; p.n1[2] = 0.0;
+    } else {
+        const double l = sqrt(dy * dy + dz * dz);
+        p.n1[0] = 0.0; p.n1[1] = dz / l; p.n1[2] = -dy / l;
+    }
+    const double il = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+    const double ux = dx * il, uy = dy * il, uz = dz * il;
+    p.n2[0] = p.n1[1] * uz - p.n1[2] * uy;
+    p.n2[1] = p.n1[2] * ux - p.n1[0] * uz;
+    p.n2[2] = p.n1[0] * uy - p.n1[1] * ux;
+    p.e1 = -(p.n1[0] * pr.ocx + p.n1[1] * pr.ocy + p.n1[2] * pr.ocz);
+    p.e2 = -(p.n2[0] * pr.ocx + p.n2[1] * pr.ocy + p.n2[2] * pr.ocz);
+    return p;
+}
+
+// FP64 continuation of a Newton solve whose FP32 residual fell into the
+// decision band at evaluation `it`: the same iteration (residual test, seeded
+// pull on a singular Jacobian, adjugate step, clamping; the seed sequence
+// continues where the FP32 loop left it) runs in double from the current
+// (u, v) for the evaluations left of max_iter, starting by re-evaluating the
+// current point in double.  Near eps the FP32 residual is at its rounding
+// floor on patches with extreme weights (its error is of the order of eps),
+// so the stop rule is applied to the FP64 residual: the solve converges, or
+// not, where the same method in double does.  Not inlined: it runs only in the
+// band, and keeps its double registers out of the FP32 loop.
+template <int P, int Q>
+__device__ __noinline__ void newton_tail_fp64(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                              float u0f, float v0f, float uf, float vf, int it, uint32_t seed,
+                                              const NewtonOpts& op, NewtonOut& o) {
+    const PlanesF64 pl = planes_fp64(r, pr);
+    const double u0 = u0f, v0 = v0f, eps = op.eps, det_eps = op.det_eps;
+    double u = uf, v = vf;
+    for (; it <= op.max_iter; ++it) {
+        double H[4], Hu[4], Hv[4], S[3], Su[3], Sv[3];
+        eval_patch_fp64<P, Q>(blk, u, v, H, Hu, Hv);
+        ++o.fp64_solves;
+        const double iw = 1.0 / H[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            S[a] = H[a] * iw;
+            Su[a] = (Hu[a] - S[a] * Hu[3]) * iw;
+            Sv[a] = (Hv[a] - S[a] * Hv[3]) * iw;
+        }
+        const double r1 = pl.n1[0] * S[0] + pl.n1[1] * S[1] + pl.n1[2] * S[2] + pl.e1;
+        const double r2 = pl.n2[0] * S[0] + pl.n2[1] * S[1] + pl.n2[2] * S[2] + pl.e2;
+        if (fabs(r1) + fabs(r2) < eps) {
+            o.evals = it;
+            o.u = (float)u; o.v = (float)v;
+            o.sx = (float)S[0]; o.sy = (float)S[1]; o.sz = (float)S[2];
+            o.ux = (float)Su[0]; o.uy = (float)Su[1]; o.uz = (float)Su[2];
+            o.vx = (float)Sv[0]; o.vy = (float)Sv[1]; o.vz = (float)Sv[2];
+            o.t = (float)((S[0] - pr.ocx) * r.dx + (S[1] - pr.ocy) * r.dy + (S[2] - pr.ocz) * r.dz);
+            return;
+        }
+        const double j11 = pl.n1[0] * Su[0] + pl.n1[1] * Su[1] + pl.n1[2] * Su[2];
+        const double j21 = pl.n2[0] * Su[0] + pl.n2[1] * Su[1] + pl.n2[2] * Su[2];
+        const double j12 = pl.n1[0] * Sv[0] + pl.n1[1] * Sv[1] + pl.n1[2] * Sv[2];
+        const double j22 = pl.n2[0] * Sv[0] + pl.n2[1] * Sv[1] + pl.n2[2] * Sv[2];
+        seed = pcg_hash(seed);
+        const double rnd1 = (double)seed * 2.3283064365386963e-10;
+        seed = pcg_hash(seed);
+        const double rnd2 = (double)seed * 2.3283064365386963e-10;
+        const double det = j11 * j22 - j12 * j21;
+        if (fabs(det) < det_eps) {
+            u = u + 0.1 * ((u0 - u) * rnd1);
+            v = v + 0.1 * ((v0 - v) * rnd2);
+        } else {
+            u = u - (j22 * r1 - j12 * r2) / det;
+            v = v - (j11 * r2 - j21 * r1) / det;
+        }
+        u = fmin(fmax(u, 0.0), 1.0);
+        v = fmin(fmax(v, 0.0), 1.0);
+    }
+    o.evals = -op.max_iter;
+    o.u = (float)u;
+    o.v = (float)v;
+}
+
 // Newton-Raphson on F(u,v) = (n1.S + e1, n2.S + e2) from (u0, v0); the
 // iteration, thresholds, seeded pull on a singular Jacobian and clamping follow
 // BezierPatchOps::newtonRhapson (src/math/bezier_patch.h:197-266).  When
 // cond_fp64 > 0 and ||J||_F^2 / |det J| exceeds it, the 2x2 solve is done in
 // FP64 (products of floats are exact there, so det J has no cancellation).
-// FINAL = false compiles the FP64 final step out (for kernels that run
-// without it, so that they carry no call to it).
+// With op.fp64_band (the FP64 final-step mode) convergence within the
+// decision band around eps is decided in FP64 (newton_tail_fp64).
+// FINAL = false compiles the FP64 final step and band out (for kernels that
+// run without them, so that they carry no call to them).
 template <int P, int Q, bool FINAL = true>
 __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
                                             float u0, float v0, uint32_t seed, const NewtonOpts& op) {
@@ -627,6 +725,7 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
     o.flat = 0;
     o.fp64_final = 0;
     float u = u0, v = v0;
+    const float accept = (FINAL && op.fp64_band) ? kBandLo * op.eps : op.eps;
     for (int it = 1; it <= op.max_iter; ++it) {
         float H[4], Hu[4], Hv[4];
         eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
@@ -636,7 +735,13 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
         const float vx = (Hv[0] - sx * Hv[3]) * iw, vy = (Hv[1] - sy * Hv[3]) * iw, vz = (Hv[2] - sz * Hv[3]) * iw;
         const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
         const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
-        if (fabsf(r1) + fabsf(r2) < op.eps) {
+        const float res = fabsf(r1) + fabsf(r2);
+        if (FINAL && op.fp64_band && res >= accept && res < kBandHi * op.eps) {
+            newton_tail_fp64<P, Q>(blk, r, pr, u0, v0, u, v, it, seed, op, o);
+            if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+            return o;
+        }
+        if (res < accept) {
             o.evals = it;
             o.u = u; o.v = v;
             o.sx = sx; o.sy = sy; o.sz = sz;

@@ -21,8 +21,12 @@ int new_scene(const nrt_build_opts& o, const ArenaLayout& L, nrt_scene** out, ch
 void finish_scene(nrt_scene* sc, const ArenaLayout& L, int N, dev::WfPlan plan, nrt_scene_info info, PatchSet&& ps,
                   int n_surfaces);
 
-// Host builder: patches already decomposed on the host.
-int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_scene** out);
+// Host builder: patches already decomposed on the host.  given: use this
+// binary tree (its order maps leaf slots to patches) instead of building one;
+// delta_by_patch: flatness per patch (input order) for flat-skip instead of
+// the computed one.
+int build_scene(PatchSet&& ps, int n_surfaces, const nrt_build_opts* opts, nrt_scene** out,
+                const BinaryBVH* given = nullptr, const float* delta_by_patch = nullptr);
 
 // Device builder.  Surfaces (nets and knots in host memory) or patches are
 // copied to the device once; decomposition, patch boxes, the binned SAH, the

@@ -38,3 +38,33 @@ def compare(gpu, patch_ref, t_ref, u_ref=None, v_ref=None):
         relb = np.abs(gpu["t"][both].astype(np.float64) - t_ref[both]) / np.abs(t_ref[both])
         st["t_rel_gt_1e-4_any"] = float((relb > 1e-4).mean())
     return st
+
+
+def root_stats(oracle_mod, P, rays_np, got, ref):
+    """Hits of the engine and of the FP64 oracle on the same rays, each refined
+    to the exact root next to it (FP64 Newton to |r1|+|r2| < 1e-11 from the
+    reported (u, v) on the reported patch; the oracle itself stops at the
+    method's eps, so its t is only good to about eps / sin(angle)).  Returns:
+    genuine (fraction of engine hits that refine to a root), t_err / uv_err
+    (engine hit against its exact root; max and quantiles), same_root
+    (fraction of rays both hit where the two exact roots coincide) and the
+    counts of rays both hit on different roots, by which one is nearer."""
+    rays = oracle_mod.Rays(*rays_np)
+    he, ho = got["patch"] >= 0, ref.patch >= 0
+    pe = oracle_mod.polish_hits(P, rays, np.where(he, got["patch"], -1), got["u"], got["v"])
+    po = oracle_mod.polish_hits(P, rays, ref.patch, ref.u, ref.v)
+    ok = he & (pe.patch >= 0)
+    st = {"genuine": float(ok.sum() / max(he.sum(), 1))}
+    if ok.any():
+        rel = np.abs(got["t"][ok].astype(np.float64) - pe.t[ok]) / np.abs(pe.t[ok])
+        duv = np.maximum(np.abs(got["u"][ok] - pe.u[ok]), np.abs(got["v"][ok] - pe.v[ok]))
+        st.update({"t_err_max": float(rel.max()), "t_err_p9999": float(np.quantile(rel, 0.9999)),
+                   "t_err_gt_1e-4": int((rel > 1e-4).sum()), "uv_err_max": float(duv.max()),
+                   "uv_err_p999": float(np.quantile(duv, 0.999))})
+    both = he & ho & (pe.patch >= 0) & (po.patch >= 0)
+    same = both & (got["patch"] == ref.patch) & (np.abs(pe.t - po.t) <= 1e-6 * np.abs(po.t))
+    st["same_root"] = float(same.sum() / max(both.sum(), 1))
+    other = both & ~same
+    st["other_root_engine_nearer"] = int((other & (pe.t < po.t)).sum())
+    st["other_root_engine_farther"] = int((other & (pe.t >= po.t)).sum())
+    return st

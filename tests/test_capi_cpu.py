@@ -36,6 +36,31 @@ def test_library_exports_header(nrt_mod):
     assert not missing, missing
 
 
+# The reference's C++ entry points (include/nrt_compat.h) under their mangled
+# names, as the reference's own declarations (src/gpu/intersect.h:9-13,
+# src/gpu/generateRaysKernel.h:6) name them.
+COMPAT_SYMBOLS = [
+    "_Z25calculateIntersectWrapperRN8SoAQueue9ray_queueEP7BVHNodeP11bezierPatchP18surfaceInteractioniiffPfPyS9_",
+    "_Z20calculateRaysWrapperRN8SoAQueue9ray_queueE10projectionR13camera_config",
+]
+
+
+def test_library_exports_reference_entry_points(nrt_mod):
+    """libnrt.so defines the reference's two C++ entry points; where the program
+    built on the reference's own headers exists (oracle/_ref/compat_driver), the
+    symbols it needs are exactly these."""
+    import ctypes
+    import subprocess
+
+    L = ctypes.CDLL(nrt_mod.lib_path())
+    assert all(hasattr(L, s) for s in COMPAT_SYMBOLS)
+    drv = os.path.join(ROOT, "oracle", "_ref", "compat_driver")
+    if os.path.exists(drv):
+        undef = subprocess.run(["nm", "-u", drv], capture_output=True, text=True, check=True).stdout
+        wanted = sorted(w for w in undef.split() if "Wrapper" in w)
+        assert wanted == sorted(COMPAT_SYMBOLS), wanted
+
+
 def test_version_and_opts(nrt_mod):
     assert b"nrt" in nrt_mod.lib().nrt_version()
     d = nrt_mod.default_opts()
