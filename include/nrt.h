@@ -75,6 +75,16 @@ int nrt_decompose(const nrt_nurbs_surface* surf, float* cp_out, float* ranges_ou
 int nrt_refine_count(const nrt_nurbs_surface* surf, float C, int* n_out, int* m_out);
 int nrt_refine_surface(const nrt_nurbs_surface* surf, float C, float* cp_out, float* u_knots_out, float* v_knots_out,
                        int* n_out, int* m_out);
+/* The same refinement computed on `device`, with the same bits: the counts by
+ * one thread per (knot span, line of the net), the A5.1 insertions by one
+ * thread per line (NurbsOps::curvatureRefinementU/V, src/math/nurbs.h:289-486,
+ * with knotsToAdd :254-281 and curveKnotInsert :96-140).  Host input and
+ * output; cp_out holds cap_points points, u_knots_out cap_u and v_knots_out
+ * cap_v floats.  *n_out, *m_out are always set; when the outputs are too small
+ * (or NULL) the call returns NRT_ERR_INVALID without writing them, so a
+ * caller can size them and call again.  Synchronous. */
+int nrt_refine_surface_device(const nrt_nurbs_surface* surf, float C, int device, float* cp_out, int64_t cap_points,
+                              float* u_knots_out, int cap_u, float* v_knots_out, int cap_v, int* n_out, int* m_out);
 
 /* Patch bounding boxes from the dehomogenised control points:
  * BezierPatchOps::bounds (src/math/bezier_patch.h:153-169).  boxes: 6 floats

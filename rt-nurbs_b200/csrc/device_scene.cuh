@@ -27,6 +27,7 @@ struct Scene {
     const float4* leafbox;   // per slot: the box of its BVH leaf (lo xyz, hi xyz in two float4), as the
                              // parent node stores it (the flat-skip's entry distance)
     int n_slots;
+    int n_nodes;             // 4-wide nodes (breadth-first: the top levels come first)
 };
 
 struct Rays {

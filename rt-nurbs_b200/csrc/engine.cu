@@ -183,6 +183,7 @@ void finish_scene(nrt_scene* sc, const ArenaLayout& L, int N, dev::WfPlan plan, 
     sc->view.obb = reinterpret_cast<const float4*>(base + L.obb);
     sc->view.leafbox = reinterpret_cast<const float4*>(base + L.leafbox);
     sc->view.n_slots = N;
+    sc->view.n_nodes = info.n_nodes;
     sc->plan = plan;
     info.n_patches = N;
     info.device_bytes = L.total;

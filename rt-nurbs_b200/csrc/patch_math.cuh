@@ -50,10 +50,20 @@ struct NewtonOpts {
     int fp64_band;   // 1: convergence near eps is decided in FP64 (newton_tail_fp64)
 };
 
-// The FP64 decision band: an FP32 residual below kBandLo * eps is accepted as
-// converged; one in [kBandLo * eps, kBandHi * eps) hands the solve to FP64,
-// which decides whether (and where) it converges within the remaining budget.
-constexpr float kBandLo = 0.125f, kBandHi = 16.f;
+// FP64 decisions of the FP64 final-step mode (op.fp64_band):
+//  * the decision band: an FP32 residual in [kBandLo * eps, kBandHi * eps)
+//    hands the solve to FP64, which continues the same iteration from there
+//    (on nets with extreme weights the FP32 residual has a rounding floor near
+//    eps and would stall in this band);
+//  * marginal outcomes: an FP32 solve that converges at one of the last
+//    kLateEvals evaluations of the budget, or that ends unconverged with its
+//    residual below kNearMiss * eps and still falling (below half the one
+//    before), is solved again in FP64 from the same start with the same seeds
+//    and budget, whose outcome stands.  Where the iteration needs the whole
+//    budget, rounding decides whether it converges in time; these are the
+//    solves on which FP32 and the same method in double part ways.
+constexpr float kBandLo = 0.25f, kBandHi = 2.f, kNearMiss = 4096.f;
+constexpr int kLateEvals = 2;
 
 struct NewtonOut {
     int evals;       // > 0 converged after this many evaluations; < 0 not converged
@@ -581,6 +591,7 @@ __device__ __noinline__ void final_step_fp64(const float* __restrict__ blk, cons
         const double det = j11 * j22 - j12 * j21;
         if (det == 0.0) break;
         const double du = (j22 * r1 - j12 * r2) / det, dv = (j11 * r2 - j21 * r1) / det;
+        const double u_at = u, v_at = v;
         const double un = fmin(fmax(u - du, 0.0), 1.0), vn = fmin(fmax(v - dv, 0.0), 1.0);
         if (fabs(un - u) + fabs(vn - v) < 1e-7) {
             // a small step: its second-order remainder is below float resolution, so the point
@@ -595,15 +606,25 @@ __device__ __noinline__ void final_step_fp64(const float* __restrict__ blk, cons
             for (int a = 0; a < 3; ++a) { bS[a] = S[a]; bSu[a] = Su[a]; bSv[a] = Sv[a]; }
             break;
         }
-        u = un;
-        v = vn;
-        eval();
-        const double res = residual(r1, r2);
-        if (!(res < best)) break;  // no progress (or a jump away): keep the best point so far
-        best = res;
-        bu = u; bv = v;
+        // the full step, else half, quarter and eighth steps (backtracking): a grazing ray's
+        // residual is far from linear over a full step, and a shorter one still makes progress
+        bool progress = false;
+        double lam = 1.0;
+#pragma unroll 1
+        for (int half = 0; half < 4 && !progress; ++half, lam *= 0.5) {
+            u = fmin(fmax(u_at - lam * du, 0.0), 1.0);
+            v = fmin(fmax(v_at - lam * dv, 0.0), 1.0);
+            eval();
+            const double res = residual(r1, r2);
+            if (res < best) {
+                progress = true;
+                best = res;
+                bu = u; bv = v;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) { bS[a] = S[a]; bSu[a] = Su[a]; bSv[a] = Sv[a]; }
+                for (int a = 0; a < 3; ++a) { bS[a] = S[a]; bSu[a] = Su[a]; bSv[a] = Sv[a]; }
+            }
+        }
+        if (!progress) break;  // keep the best point so far
     }
     u = bu; v = bv;
 #pragma unroll
@@ -725,7 +746,16 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
     o.flat = 0;
     o.fp64_final = 0;
     float u = u0, v = v0;
-    const float accept = (FINAL && op.fp64_band) ? kBandLo * op.eps : op.eps;
+    const uint32_t seed0 = seed;
+    const bool band = FINAL && op.fp64_band;
+    const float accept = band ? kBandLo * op.eps : op.eps;
+    float res_prev = INFINITY, res_last = INFINITY;
+    // the whole solve again in FP64, from the same start with the same seeds
+    auto resolve_fp64 = [&]() {
+        newton_tail_fp64<P, Q>(blk, r, pr, u0, v0, u0, v0, 1, seed0, op, o);
+        if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+        return o;
+    };
     for (int it = 1; it <= op.max_iter; ++it) {
         float H[4], Hu[4], Hv[4];
         eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
@@ -736,11 +766,14 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
         const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
         const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
         const float res = fabsf(r1) + fabsf(r2);
-        if (FINAL && op.fp64_band && res >= accept && res < kBandHi * op.eps) {
+        res_prev = res_last;
+        res_last = res;
+        if (band && res >= accept && res < kBandHi * op.eps) {
             newton_tail_fp64<P, Q>(blk, r, pr, u0, v0, u, v, it, seed, op, o);
             if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
             return o;
         }
+        if (band && res < accept && it > op.max_iter - kLateEvals) return resolve_fp64();
         if (res < accept) {
             o.evals = it;
             o.u = u; o.v = v;
@@ -777,6 +810,7 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
         u = fminf(fmaxf(u, 0.f), 1.f);
         v = fminf(fmaxf(v, 0.f), 1.f);
     }
+    if (band && res_last < kNearMiss * op.eps && res_last < 0.5f * res_prev) return resolve_fp64();
     o.evals = -op.max_iter;
     o.u = u; o.v = v;
     return o;

@@ -24,64 +24,19 @@
 #include <vector>
 
 #include "nrt_internal.h"
+#include "refine_math.h"
 
 namespace nrt {
 
 namespace {
 
-struct V3 {
-    float x, y, z;
-};
+using refine_math::V3;
 struct Q4 {
     float x, y, z, w;
 };
 
-V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-V3 scale(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
-float norm(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
-
-// Algorithm A2.1: the span index of u in U (n+1 control points, degree p).
-int find_span(int n, int p, float u, const float* U) {
-    if (u == U[n + 1]) return n;
-    int lo = p, hi = n + 1, mid = (lo + hi) / 2;
-    while (u < U[mid] || u >= U[mid + 1]) {
-        if (u < U[mid]) hi = mid;
-        else lo = mid;
-        mid = (lo + hi) / 2;
-    }
-    return mid;
-}
-
-// How many times u occurs at or below index k.
-int multiplicity_at(const float* U, int k, float u) {
-    int s = 0;
-    for (int i = k; i >= 0 && U[i] == u; --i) ++s;
-    return s;
-}
-
-// Knots to insert into span i of the curve P (dehomogenised), degree p.
-int knot_count(const V3* P, const float* U, int i, float C, int p) {
-    V3 Vj[NRT_MAX_DEGREE + 1];
-    float vsum = 0.f;
-    const int base = i - p + 1;
-    for (int j = base; j <= i; ++j) {
-        const float d = U[j + p] - U[j];
-        Vj[j - base] = d > 0.f ? scale(sub(P[j], P[j - 1]), p / d) : V3{0.f, 0.f, 0.f};
-        vsum += norm(Vj[j - base]);
-    }
-    float amax = 0.f;
-    for (int j = base + 1; j <= i; ++j) {
-        const float d = U[j + p - 1] - U[j];
-        const V3 A = d > 0.f ? scale(sub(Vj[j - base], Vj[j - 1 - base]), (p - 1) / d) : V3{0.f, 0.f, 0.f};
-        amax = std::fmax(amax, norm(A));
-    }
-    const float num = amax * powf(U[i + 1] - U[i], 1.5f);
-    const float den = sqrtf(vsum / p);
-    if (!(den > 1e-9f)) return 0;
-    const float nf = C * num / den;
-    if (!(nf > 1e-9f)) return 0;
-    return nf < (float)(1 << 20) ? (int)nf : (1 << 20);
-}
+using refine_math::find_span;
+using refine_math::multiplicity_at;
 
 // Algorithm A5.1 with r = 1: insert u (span k, multiplicity s < p) into the
 // curve Pw (np+1 points, knots UP) giving Qw (np+2 points) and UQ.
@@ -122,7 +77,8 @@ void refine_dir(std::vector<Q4>& net, int& rows, int& cols, std::vector<float>& 
                 const Q4& q = along_u ? at(a, l) : at(l, a);
                 curve[a] = {q.x / q.w, q.y / q.w, q.z / q.w};
             }
-            ni = std::max(ni, knot_count(curve.data(), K.data(), i, C, deg));
+            const V3* P = curve.data();
+            ni = std::max(ni, refine_math::knot_count([P](int a) { return P[a]; }, K.data(), i, C, deg));
         }
         add[i - deg] = ni;
     }

@@ -46,12 +46,6 @@ __device__ __forceinline__ float key_t(unsigned long long key) {
     return key == kNoHit ? INFINITY : __uint_as_float((unsigned)(key >> 32));
 }
 
-__device__ __forceinline__ void load_ray(const Rays& rays, long long i, RayFrame& r) {
-    r.ox = __ldg(rays.ox + i); r.oy = __ldg(rays.oy + i); r.oz = __ldg(rays.oz + i);
-    r.dx = __ldg(rays.dx + i); r.dy = __ldg(rays.dy + i); r.dz = __ldg(rays.dz + i);
-    ray_planes(r);
-}
-
 // Warp-aggregated increment of hist[key]: lanes with equal keys add once.
 __device__ __forceinline__ int aggregated_add(int* hist, int key) {
     const unsigned active = __activemask();
@@ -70,14 +64,33 @@ struct StepTally {
     unsigned long long boxes, cands, culled, err;
 };
 
+// The top of the 4-wide tree staged in shared memory by every traversal
+// block: the tree is laid out breadth first, so its first kStagedNodes nodes
+// are its top levels (1 + 4 + 16 + 64 nodes: four levels, 10.9 KB), which
+// every ray visits.
+constexpr int kStagedNodes = 85;
+
+__device__ __forceinline__ int stage_nodes(const Scene& sc, float4* smem) {
+    const int k = sc.n_nodes < kStagedNodes ? sc.n_nodes : kStagedNodes;
+    const float4* src = reinterpret_cast<const float4*>(sc.nodes);
+    for (int i = threadIdx.x; i < 8 * k; i += blockDim.x) smem[i] = __ldg(src + i);
+    __syncthreads();
+    return k;
+}
+
 // One active ray j (ray index i) for one round: resume its saved stack, emit
 // up to `quota` leaf patches, save the stack, and queue the ray for the next
-// round if its stack is not empty.
-__device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long long n, int round, int j, long long i,
-                                         int quota, const Opts& op, const WfBuffers& wb, int cur, int32_t* tests,
-                                         const int32_t* rank_of, StepTally& c) {
+// round if its stack is not empty.  Children of an inner node are visited
+// nearest first: the nearest is entered directly and the others pushed
+// (farthest first), which visits nodes in the same order as pushing all of
+// them and popping the top, without the round trip through the stack.
+__device__ __forceinline__ void step_ray(const Scene& sc, const float4* __restrict__ top, int n_top, const Rays& rays,
+                                         long long n, int round, int j, long long i, int quota, const Opts& op,
+                                         const WfBuffers& wb, int cur, int32_t* tests, const int32_t* rank_of,
+                                         StepTally& c) {
     RayFrame r;
-    load_ray(rays, i, r);
+    r.ox = __ldg(rays.ox + i); r.oy = __ldg(rays.oy + i); r.oz = __ldg(rays.oz + i);
+    r.dx = __ldg(rays.dx + i); r.dy = __ldg(rays.dy + i); r.dz = __ldg(rays.dz + i);
     const float rdx = __frcp_rn(r.dx), rdy = __frcp_rn(r.dy), rdz = __frcp_rn(r.dz);
     int st[kStack];
     float stt[kStack];
@@ -100,17 +113,29 @@ __device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long
     }
     int32_t* emit = wb.emit_slot + (long long)j * kEmitMax;
     int emitted = 0;
-    while (sp > 0 && emitted < quota) {
-        --sp;
-        const int ref = st[sp];
-        const float te = stt[sp];
-        if (te >= best) continue;
+    int ref = 0;          // the node to visit next: the nearest child just entered, or a popped entry
+    bool have = false;    // ref holds a child entered directly
+    while (have || (sp > 0 && emitted < quota)) {
+        if (!have) {
+            --sp;
+            ref = st[sp];
+            if (stt[sp] >= best) continue;
+        }
+        have = false;
         if (ref >= 0) {
-            const float4* nd = reinterpret_cast<const float4*>(sc.nodes + ref);
-            const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
-            const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
-            const int4 ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
-            const int4 cn = __ldg(reinterpret_cast<const int4*>(nd + 7));
+            const float4* nd = ref < n_top ? top + 8 * ref : reinterpret_cast<const float4*>(sc.nodes + ref);
+            float4 lx, hx, ly, hy, lz, hz;
+            int4 ch, cn;
+            if (ref < n_top) {
+                lx = nd[0]; hx = nd[1]; ly = nd[2]; hy = nd[3]; lz = nd[4]; hz = nd[5];
+                ch = reinterpret_cast<const int4*>(nd)[6];
+                cn = reinterpret_cast<const int4*>(nd)[7];
+            } else {
+                lx = __ldg(nd + 0); hx = __ldg(nd + 1); ly = __ldg(nd + 2); hy = __ldg(nd + 3);
+                lz = __ldg(nd + 4); hz = __ldg(nd + 5);
+                ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
+                cn = __ldg(reinterpret_cast<const int4*>(nd + 7));
+            }
             const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
             const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
             const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
@@ -128,18 +153,26 @@ __device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long
                     ++k;
                 }
             }
-            for (int a = 1; a < k; ++a)  // farthest pushed first: nearest popped next
+            for (int a = 1; a < k; ++a)  // descending entry distance (stable): the nearest last
                 for (int b = a; b > 0 && tt[b] > tt[b - 1]; --b) {
                     const float tf = tt[b]; tt[b] = tt[b - 1]; tt[b - 1] = tf;
                     const int rf = rr[b]; rr[b] = rr[b - 1]; rr[b - 1] = rf;
                 }
-            for (int a = 0; a < k; ++a) {
-                if (sp < kStack) {
-                    st[sp] = rr[a];
-                    stt[sp] = tt[a];
-                    ++sp;
+            if (k > 0) {
+                for (int a = 0; a + 1 < k; ++a) {
+                    if (sp < kStack) {
+                        st[sp] = rr[a];
+                        stt[sp] = tt[a];
+                        ++sp;
+                    } else {
+                        ++c.err;  // stack overflow: the subtree is dropped and the error counted
+                    }
+                }
+                if (sp < kStack) {  // the nearest child: entered next (it would have been pushed, then popped)
+                    ref = rr[k - 1];
+                    have = true;
                 } else {
-                    ++c.err;  // stack overflow: the subtree is dropped and the error counted
+                    ++c.err;
                 }
             }
         } else {
@@ -183,11 +216,13 @@ __device__ __forceinline__ void step_count(unsigned long long* ctr, const Opts& 
 __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long n, int round, int n_active,
                                                  int quota, Opts op, WfBuffers wb, int cur, int32_t* tests,
                                                  unsigned long long* ctr, const int32_t* rank_of) {
+    __shared__ float4 top[8 * kStagedNodes];
+    const int n_top = stage_nodes(sc, top);
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     StepTally c{};
     if (j < n_active)
-        step_ray(sc, rays, n, round, j, round == 0 ? (long long)j : (long long)wb.active[cur][j], quota, op, wb, cur,
-                 tests, rank_of, c);
+        step_ray(sc, top, n_top, rays, n, round, j, round == 0 ? (long long)j : (long long)wb.active[cur][j], quota,
+                 op, wb, cur, tests, rank_of, c);
     step_count(ctr, op, (round == 0 && j < n_active) ? 1ull : 0ull, c);
 }
 
@@ -203,6 +238,8 @@ __global__ void __launch_bounds__(128) k_wf_step_dev(Scene sc, Rays rays, long l
     const int round = wb.counts[2], cur = round & 1;
     const int n_active = round == 0 ? (int)n : wb.counts[cur];
     const int quota = round_quota(round, quota0, quota_max);
+    __shared__ float4 top[8 * kStagedNodes];
+    const int n_top = stage_nodes(sc, top);
     const int lane = threadIdx.x & 31;
     StepTally c{};
     unsigned long long seen = 0;
@@ -213,8 +250,8 @@ __global__ void __launch_bounds__(128) k_wf_step_dev(Scene sc, Rays rays, long l
         if (base >= n_active) break;
         const int j = base + lane;
         if (j < n_active) {
-            step_ray(sc, rays, n, round, j, round == 0 ? (long long)j : (long long)wb.active[cur][j], quota, op, wb,
-                     cur, tests, rank_of, c);
+            step_ray(sc, top, n_top, rays, n, round, j, round == 0 ? (long long)j : (long long)wb.active[cur][j],
+                     quota, op, wb, cur, tests, rank_of, c);
             ++seen;
         }
     }

@@ -27,6 +27,7 @@ from .lib import (  # noqa: F401
     shade,
     write_ppm,
     refine,
+    refine_device,
     INIT_BILINEAR,
     INIT_LEARNED,
     INIT_MIDPOINT,

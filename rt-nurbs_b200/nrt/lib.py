@@ -146,6 +146,8 @@ def lib():
         L.nrt_refine_count.argtypes = [C.POINTER(NurbsSurface), C.c_float, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.nrt_refine_surface.argtypes = [C.POINTER(NurbsSurface), C.c_float, vp, vp, vp, C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]
+        L.nrt_refine_surface_device.argtypes = [C.POINTER(NurbsSurface), C.c_float, C.c_int, vp, C.c_int64, vp, C.c_int,
+                                                vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.nrt_bounce_scratch_bytes.argtypes = [C.c_int64]
         L.nrt_bounce_scratch_bytes.restype = C.c_size_t
         L.nrt_generate_bounce_rays.argtypes = [C.POINTER(RaysC), C.POINTER(HitsC), C.c_int64, C.c_uint32, C.c_float,
@@ -212,6 +214,25 @@ def refine(s, c: float):
     V = np.zeros(m.value + s.q + 2, np.float32)
     _check(L.nrt_refine_surface(C.byref(st), float(c), cp.ctypes.data, U.ctypes.data, V.ctypes.data, C.byref(n),
                                 C.byref(m)))
+    return Surface(cp, U, V, n.value, m.value, s.p, s.q)
+
+
+def refine_device(s, c: float, device: int = 0):
+    """nrt_refine_surface_device: the same refinement computed on the GPU."""
+    from .scenes import Surface
+
+    L = lib()
+    st, keep = _surface_struct(s)
+    n, m = C.c_int(), C.c_int()
+    rc = L.nrt_refine_surface_device(C.byref(st), float(c), int(device), None, 0, None, 0, None, 0, C.byref(n),
+                                     C.byref(m))
+    if rc not in (0, 1) or n.value < 0:
+        _check(rc)
+    cp = np.zeros(((n.value + 1) * (m.value + 1), 4), np.float32)
+    U = np.zeros(n.value + s.p + 2, np.float32)
+    V = np.zeros(m.value + s.q + 2, np.float32)
+    _check(L.nrt_refine_surface_device(C.byref(st), float(c), int(device), cp.ctypes.data, cp.shape[0],
+                                       U.ctypes.data, U.size, V.ctypes.data, V.size, C.byref(n), C.byref(m)))
     return Surface(cp, U, V, n.value, m.value, s.p, s.q)
 
 
