@@ -84,6 +84,7 @@ __device__ __forceinline__ bool flat_accept(const float* __restrict__ blk, const
     o.fp64_solves = 0;
     o.fp64_final = 0;
     o.flat = 1;
+    o.done = 1;  // the one evaluation at the guess
     return true;
 }
 

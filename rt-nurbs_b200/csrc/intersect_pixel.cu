@@ -51,10 +51,10 @@ __device__ __forceinline__ void test_patch(const Scene& sc, int slot, const RayF
     }
     const NewtonOut o = newton<P, Q, FINAL>(blk, r, pr, gu, gv, seed, op.nw);
     ++c.solves;
-    c.evals += (unsigned long long)(o.evals > 0 ? o.evals : -o.evals);
+    c.evals += (unsigned long long)o.done;
     c.f64s += (unsigned long long)o.fp64_solves;
     c.f64f += (unsigned long long)o.fp64_final;
-    if (op.counters) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, (unsigned long long)(o.evals > 0 ? o.evals : -o.evals));
+    if (op.counters) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, (unsigned long long)o.done);
     if (o.evals > 0 && 0.f < o.t && o.t < b.t_max) {
         b.t_max = o.t;
         b.slot = slot;

@@ -55,6 +55,7 @@ struct nrt_mlp {
     float* v = nullptr;
     float* grad = nullptr;
     float* loss = nullptr;    // device scalar
+    int* err = nullptr;       // device word: the training kernel gave up waiting for its tensor cores
     void* blob = nullptr;     // device, kernel layout
     long long step = 0;
     std::vector<float> host_m, host_v;  // only used by save/load staging
@@ -489,6 +490,8 @@ int nrt_mlp_create(int device, uint32_t seed, nrt_mlp** out) {
     if (e == cudaSuccess) e = cudaMalloc(&m->v, pbytes);
     if (e == cudaSuccess) e = cudaMalloc(&m->grad, pbytes);
     if (e == cudaSuccess) e = cudaMalloc(&m->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(m->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&m->blob, kBlobBytes);
     if (e == cudaSuccess) e = cudaMemset(m->blob, 0, kBlobBytes);
     if (e == cudaSuccess) e = cudaMemset(m->m, 0, pbytes);
@@ -532,6 +535,7 @@ int nrt_mlp_destroy(nrt_mlp* m) {
     cudaFree(m->v);
     cudaFree(m->grad);
     cudaFree(m->loss);
+    cudaFree(m->err);
     cudaFree(m->blob);
     delete m;
     return NRT_OK;
@@ -569,20 +573,24 @@ int nrt_mlp_forward(const nrt_mlp* m, const float* features, int64_t n, float* o
     return e == cudaSuccess ? NRT_OK : cuda_fail(e, "mlp forward");
 }
 
+// Forward + backward of one batch on the tcgen05 tensor cores (mlp_tc.cu).
 static int fwd_bwd(nrt_mlp* m, const float* X, const float* T, const int32_t* perm, long long begin, long long count,
                    long long batch, cudaStream_t st) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_mlp_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
-        attr_set = true;
-    }
-    const long long tiles = (count + 31) / 32;
-    long long blocks = (tiles + 3) / 4;
-    if (blocks > 148) blocks = 148;
-    k_mlp_fwd_bwd<<<(unsigned)blocks, 128, sizeof(TrainSmem), st>>>(nrt::blob_params(m->blob), X, T, perm, begin, count,
-                                                                      1.f / (float)batch, m->grad, m->loss);
-    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e = nrt::dev::launch_mlp_fwd_bwd_tc(nrt::blob_params(m->blob), X, T, perm, begin, count,
+                                                          1.f / (float)batch, m->grad, m->loss, m->err, st);
     return e == cudaSuccess ? NRT_OK : cuda_fail(e, "mlp fwd/bwd");
+}
+
+// After a synchronisation: did a training kernel give up waiting for its tensor cores?
+static int check_err(nrt_mlp* m) {
+    int h = 0;
+    const cudaError_t e = cudaMemcpy(&h, m->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp error word");
+    if (h) {
+        cudaMemset(m->err, 0, sizeof(int));
+        return nrt::fail(NRT_ERR_DEVICE, "mlp training: a tensor-core step did not complete within its wait limit");
+    }
+    return NRT_OK;
 }
 
 int nrt_mlp_gradients(nrt_mlp* m, const float* features, const float* targets, int64_t n, float* host_grads,
@@ -600,6 +608,7 @@ int nrt_mlp_gradients(nrt_mlp* m, const float* features, const float* targets, i
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaMemsetAsync(m->grad, 0, sizeof(float) * kNumParams, st);
     if (e != cudaSuccess) return cuda_fail(e, "mlp gradients");
+    if (int s3 = check_err(m)) return s3;
     if (host_loss) *host_loss = loss;
     return NRT_OK;
 }
@@ -640,6 +649,7 @@ int nrt_mlp_train(nrt_mlp* m, const float* features, const float* targets, int64
         e = cudaMemcpyAsync(&loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) { status = cuda_fail(e, "epoch loss"); break; }
+        if ((status = check_err(m)) != NRT_OK) break;
         if (host_epoch_loss) host_epoch_loss[epoch] = loss / (float)batches;
     }
     cudaFree(perm);

@@ -114,6 +114,13 @@ __device__ __forceinline__ void features(const PatchFrame& f, int p, int q, cons
     for (int k = 0; k < 6; ++k) x[k] = fminf(fmaxf(x[k], -8.f), 8.f);  // keep far-outside inputs bounded
 }
 
+// Forward + backward of one training batch on the tcgen05 tensor cores
+// (mlp_tc.cu): gradients added to grad (public parameter order), the batch
+// loss to *loss; *err set if a tensor-core step did not complete.
+cudaError_t launch_mlp_fwd_bwd_tc(const MlpParams& P, const float* X, const float* T, const int32_t* perm,
+                                  long long begin, long long count, float inv_batch, float* grad, float* loss, int* err,
+                                  cudaStream_t st);
+
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<const uint32_t*>(&v);

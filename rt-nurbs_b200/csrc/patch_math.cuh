@@ -73,6 +73,7 @@ struct NewtonOut {
     int fp64_solves;
     int fp64_final;
     int flat;        // 1: accepted by the flat-skip test at the initial guess (evals 0)
+    int done;        // FP32 evaluations actually run (the fixed-point exit ends some solves early)
 };
 
 // PCG hash (src/math/math_utils.h:12-17).
@@ -530,11 +531,12 @@ __device__ __forceinline__ bool obb_misses(const float4* __restrict__ obb, const
 
 // FP64 refinement of a converged (u, v): the ray's planes are rebuilt in
 // double from the (float) ray (the FP32 planes are off the ray by an
-// ulp-sized angle, which a grazing ray turns into a t shift), then up to six
-// Newton steps in double (near-singular Jacobians of grazing rays converge
-// slowly), each re-evaluating the patch, for as long as the residual
-// decreases; the point with the smallest residual is kept, so the step never
-// makes a converged FP32 hit worse.  A step below 1e-7 in (u, v) ends the
+// ulp-sized angle, which a grazing ray turns into a t shift), then up to 16
+// Newton steps in double (a ray that nearly touches the surface has two
+// crossings close together, where Newton converges only linearly), each
+// re-evaluating the patch, for as long as the residual decreases (a full step,
+// else a half, quarter or eighth of it); the point with the smallest residual
+// is kept, so the step never makes a converged FP32 hit worse.  A step below 1e-7 in (u, v) ends the
 // refinement with a first-order move of S (no further evaluation): that is
 // the common case, one FP64 evaluation per hit.  S, dS/du, dS/dv and t are
 // those of the final (u, v), in double.  Not inlined: every caller (Newton on
@@ -583,7 +585,7 @@ __device__ __noinline__ void final_step_fp64(const float* __restrict__ blk, cons
     double best = residual(r1, r2);
     double bu = u, bv = v, bS[3] = {S[0], S[1], S[2]}, bSu[3] = {Su[0], Su[1], Su[2]}, bSv[3] = {Sv[0], Sv[1], Sv[2]};
 #pragma unroll 1
-    for (int it = 0; it < 6 && best > 0.0; ++it) {
+    for (int it = 0; it < 16 && best > 0.0; ++it) {
         const double j11 = n1[0] * Su[0] + n1[1] * Su[1] + n1[2] * Su[2];
         const double j21 = n2[0] * Su[0] + n2[1] * Su[1] + n2[2] * Su[2];
         const double j12 = n1[0] * Sv[0] + n1[1] * Sv[1] + n1[2] * Sv[2];
@@ -735,84 +737,147 @@ __device__ __noinline__ void newton_tail_fp64(const float* __restrict__ blk, con
 // cond_fp64 > 0 and ||J||_F^2 / |det J| exceeds it, the 2x2 solve is done in
 // FP64 (products of floats are exact there, so det J has no cancellation).
 // With op.fp64_band (the FP64 final-step mode) convergence within the
-// decision band around eps is decided in FP64 (newton_tail_fp64).
-// FINAL = false compiles the FP64 final step and band out (for kernels that
-// run without them, so that they carry no call to them).
+// decision band around eps, and the marginal outcomes, are decided in FP64
+// (newton_tail_fp64).  FINAL = false compiles the FP64 final step and the FP64
+// decisions out (for kernels that run without them, so that they carry no
+// call to them).
+//
+// The solve is a state machine advanced one evaluation at a time
+// (newton_step), so that a kernel can run the evaluations of many solves in
+// lockstep and give a lane a new solve as soon as its own ends; newton() runs
+// one solve to its end.  One early exit is added, exact: when a regular
+// Newton step (not the seeded pull) leaves the clamped iterate unchanged, the
+// next evaluation would repeat this one, with the same residual and step,
+// until the budget runs out, so the solve ends there unconverged (evals counts
+// the evaluations actually run; the outcome, -max_iter, is unchanged).
+struct NewtonState {
+    float u, v, u0, v0;
+    float res_prev, res_last;
+    uint32_t seed, seed0;
+    int it;      // the evaluation about to run, 1-based
+    int done;    // evaluations run
+    int f64;     // 2x2 steps solved in FP64 so far
+};
+
+__device__ __forceinline__ NewtonState newton_start(float u0, float v0, uint32_t seed) {
+    NewtonState s;
+    s.u = u0; s.v = v0; s.u0 = u0; s.v0 = v0;
+    s.res_prev = INFINITY; s.res_last = INFINITY;
+    s.seed = seed; s.seed0 = seed;
+    s.it = 1;
+    s.done = 0;
+    s.f64 = 0;
+    return s;
+}
+
+// One evaluation (and step) of the solve in s.  Returns true when the solve
+// has ended, with o holding its outcome (o is written only then).
+template <int P, int Q, bool FINAL = true>
+__device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                            NewtonState& s, const NewtonOpts& op, NewtonOut& o) {
+    const bool band = FINAL && op.fp64_band;
+    const float accept = band ? kBandLo * op.eps : op.eps;
+    auto end = [&]() {
+        o.fp64_solves = s.f64;
+        o.flat = 0;
+        o.fp64_final = 0;
+        o.done = s.done;
+    };
+    if (s.it > op.max_iter) {  // no evaluation left (max_iter <= 0)
+        end();
+        o.evals = -op.max_iter;
+        o.u = s.u; o.v = s.v;
+        return true;
+    }
+    // the whole solve again in FP64, from the same start with the same seeds
+    auto resolve_fp64 = [&]() {
+        newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, s.u0, s.v0, 1, s.seed0, op, o);
+        if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+    };
+    const float u = s.u, v = s.v;
+    float H[4], Hu[4], Hv[4];
+    eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
+    ++s.done;
+    const float iw = __frcp_rn(H[3]);
+    const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
+    const float ux = (Hu[0] - sx * Hu[3]) * iw, uy = (Hu[1] - sy * Hu[3]) * iw, uz = (Hu[2] - sz * Hu[3]) * iw;
+    const float vx = (Hv[0] - sx * Hv[3]) * iw, vy = (Hv[1] - sy * Hv[3]) * iw, vz = (Hv[2] - sz * Hv[3]) * iw;
+    const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
+    const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
+    const float res = fabsf(r1) + fabsf(r2);
+    s.res_prev = s.res_last;
+    s.res_last = res;
+    if (band && res >= accept && res < kBandHi * op.eps) {
+        end();
+        newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, u, v, s.it, s.seed, op, o);
+        if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+        return true;
+    }
+    if (band && res < accept && s.it > op.max_iter - kLateEvals) {
+        end();
+        resolve_fp64();
+        return true;
+    }
+    if (res < accept) {
+        end();
+        o.evals = s.it;
+        o.u = u; o.v = v;
+        o.sx = sx; o.sy = sy; o.sz = sz;
+        o.ux = ux; o.uy = uy; o.uz = uz;
+        o.vx = vx; o.vy = vy; o.vz = vz;
+        o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
+        if (FINAL && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+        return true;
+    }
+    const float j11 = r.n1x * ux + r.n1y * uy + r.n1z * uz;
+    const float j21 = r.n2x * ux + r.n2y * uy + r.n2z * uz;
+    const float j12 = r.n1x * vx + r.n1y * vy + r.n1z * vz;
+    const float j22 = r.n2x * vx + r.n2y * vy + r.n2z * vz;
+    s.seed = pcg_hash(s.seed);
+    const float rnd1 = (float)s.seed * 2.3283064e-10f;
+    s.seed = pcg_hash(s.seed);
+    const float rnd2 = (float)s.seed * 2.3283064e-10f;
+    const float det = j11 * j22 - j12 * j21;
+    float un, vn;
+    const bool pull = fabsf(det) < op.det_eps;
+    if (pull) {
+        un = u + 0.1f * ((s.u0 - u) * rnd1);
+        vn = v + 0.1f * ((s.v0 - v) * rnd2);
+    } else if (op.cond_fp64 > 0.f &&
+               (j11 * j11 + j12 * j12 + j21 * j21 + j22 * j22) > op.cond_fp64 * fabsf(det)) {
+        const double dd = (double)j11 * j22 - (double)j12 * j21;
+        un = (float)((double)u - ((double)j22 * r1 - (double)j12 * r2) / dd);
+        vn = (float)((double)v - ((double)j11 * r2 - (double)j21 * r1) / dd);
+        ++s.f64;
+    } else {
+        const float id = __frcp_rn(det);
+        un = u - (j22 * r1 - j12 * r2) * id;
+        vn = v - (j11 * r2 - j21 * r1) * id;
+    }
+    s.u = fminf(fmaxf(un, 0.f), 1.f);
+    s.v = fminf(fmaxf(vn, 0.f), 1.f);
+    ++s.it;
+    const bool stuck = !pull && s.u == u && s.v == v;  // a fixed point of the iteration
+    if (s.it > op.max_iter || stuck) {
+        end();
+        if (!stuck && band && s.res_last < kNearMiss * op.eps && s.res_last < 0.5f * s.res_prev) {
+            resolve_fp64();
+            return true;
+        }
+        o.evals = -op.max_iter;
+        o.u = s.u; o.v = s.v;
+        return true;
+    }
+    return false;
+}
+
 template <int P, int Q, bool FINAL = true>
 __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
                                             float u0, float v0, uint32_t seed, const NewtonOpts& op) {
     NewtonOut o;
-    o.fp64_solves = 0;
-    o.flat = 0;
-    o.fp64_final = 0;
-    float u = u0, v = v0;
-    const uint32_t seed0 = seed;
-    const bool band = FINAL && op.fp64_band;
-    const float accept = band ? kBandLo * op.eps : op.eps;
-    float res_prev = INFINITY, res_last = INFINITY;
-    // the whole solve again in FP64, from the same start with the same seeds
-    auto resolve_fp64 = [&]() {
-        newton_tail_fp64<P, Q>(blk, r, pr, u0, v0, u0, v0, 1, seed0, op, o);
-        if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
-        return o;
-    };
-    for (int it = 1; it <= op.max_iter; ++it) {
-        float H[4], Hu[4], Hv[4];
-        eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
-        const float iw = __frcp_rn(H[3]);
-        const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
-        const float ux = (Hu[0] - sx * Hu[3]) * iw, uy = (Hu[1] - sy * Hu[3]) * iw, uz = (Hu[2] - sz * Hu[3]) * iw;
-        const float vx = (Hv[0] - sx * Hv[3]) * iw, vy = (Hv[1] - sy * Hv[3]) * iw, vz = (Hv[2] - sz * Hv[3]) * iw;
-        const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
-        const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
-        const float res = fabsf(r1) + fabsf(r2);
-        res_prev = res_last;
-        res_last = res;
-        if (band && res >= accept && res < kBandHi * op.eps) {
-            newton_tail_fp64<P, Q>(blk, r, pr, u0, v0, u, v, it, seed, op, o);
-            if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
-            return o;
-        }
-        if (band && res < accept && it > op.max_iter - kLateEvals) return resolve_fp64();
-        if (res < accept) {
-            o.evals = it;
-            o.u = u; o.v = v;
-            o.sx = sx; o.sy = sy; o.sz = sz;
-            o.ux = ux; o.uy = uy; o.uz = uz;
-            o.vx = vx; o.vy = vy; o.vz = vz;
-            o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
-            if (FINAL && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
-            return o;
-        }
-        const float j11 = r.n1x * ux + r.n1y * uy + r.n1z * uz;
-        const float j21 = r.n2x * ux + r.n2y * uy + r.n2z * uz;
-        const float j12 = r.n1x * vx + r.n1y * vy + r.n1z * vz;
-        const float j22 = r.n2x * vx + r.n2y * vy + r.n2z * vz;
-        seed = pcg_hash(seed);
-        const float rnd1 = (float)seed * 2.3283064e-10f;
-        seed = pcg_hash(seed);
-        const float rnd2 = (float)seed * 2.3283064e-10f;
-        const float det = j11 * j22 - j12 * j21;
-        if (fabsf(det) < op.det_eps) {
-            u = u + 0.1f * ((u0 - u) * rnd1);
-            v = v + 0.1f * ((v0 - v) * rnd2);
-        } else if (op.cond_fp64 > 0.f &&
-                   (j11 * j11 + j12 * j12 + j21 * j21 + j22 * j22) > op.cond_fp64 * fabsf(det)) {
-            const double dd = (double)j11 * j22 - (double)j12 * j21;
-            u = (float)((double)u - ((double)j22 * r1 - (double)j12 * r2) / dd);
-            v = (float)((double)v - ((double)j11 * r2 - (double)j21 * r1) / dd);
-            ++o.fp64_solves;
-        } else {
-            const float id = __frcp_rn(det);
-            u = u - (j22 * r1 - j12 * r2) * id;
-            v = v - (j11 * r2 - j21 * r1) * id;
-        }
-        u = fminf(fmaxf(u, 0.f), 1.f);
-        v = fminf(fmaxf(v, 0.f), 1.f);
+    NewtonState s = newton_start(u0, v0, seed);
+    while (!newton_step<P, Q, FINAL>(blk, r, pr, s, op, o)) {
     }
-    if (band && res_last < kNearMiss * op.eps && res_last < 0.5f * res_prev) return resolve_fp64();
-    o.evals = -op.max_iter;
-    o.u = u; o.v = v;
     return o;
 }
 
