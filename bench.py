@@ -364,7 +364,12 @@ def nrt_arm(args):
                          "vs_plain_pixel": round(ms_plain / ms_learned, 3), "agreement": agree,
                          "newton_evals_per_ray": round(lc["newton_evals"] / lc["rays"], 3),
                          "learned_solves_per_ray": round(lc["learned_solves"] / lc["rays"], 3),
-                         "fallback_rate": round(lc["learned_fallbacks"] / max(1, lc["learned_solves"]), 4)}
+                         "fallback_rate": round(lc["learned_fallbacks"] / max(1, lc["learned_solves"]), 4),
+                         # over the pairs that have a root (the guess's solve or the plain fallback converged)
+                         "fallback_rate_rooted": round(lc["learned_fallback_converged"] /
+                                                       max(1, lc["learned_converged"] + lc["learned_fallback_converged"]),
+                                                       4),
+                         "vs_plain_wavefront": None}
     except Exception as exc:  # reported, never silently replaced
         learned_block = {"error": str(exc)[:200]}
 
@@ -512,6 +517,8 @@ def nrt_arm(args):
             dt, m = cb["run"](cb["idx"])
             cpu = {"value": round(m / dt / 1e6, 4), "unit": "Mrays/s", "cores": cb["cores"], "kind": cb["kind"],
                    "sample": cb["sample"]}
+        if learned_block and "ms_per_step" in learned_block:
+            learned_block["vs_plain_wavefront"] = round(ms_step / learned_block["ms_per_step"], 3)
         line = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and rays)",
@@ -530,6 +537,8 @@ def nrt_arm(args):
                                "fp64_solve_frac": round(cnt["fp64_solves"] / max(1, cnt["newton_evals"]), 5),
                                "hit_rate": round(cnt["hits"] / cnt["rays"], 4),
                                "wavefront_rounds": cnt["rounds"], "kernels_per_step": cnt["kernel_launches"]},
+                "value_path": "plain-init wavefront (the product): the learned-init wavefront is slower on this "
+                              "workload and reported in learned_init_wavefront with its ratio to it",
                 "speedup_vs_plain_pixel": round(ms_plain / ms_step, 3),
                 "learned_init_wavefront": learned_block,
                 "precision_stress": prec_block,

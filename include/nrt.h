@@ -254,13 +254,17 @@ typedef struct {
     int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 540 bytes per ray) */
     int32_t quota0;          /* candidates a ray emits in the first round, doubling per round ... */
     int32_t quota_max;       /* ... up to this many (<= 8); the default 4, then 8 */
+    int32_t newton_refill;   /* Newton kernels of the plain solve: a warp gives its idle lanes new
+                                solves once this many (1..32) are idle; 32 = only when all are idle
+                                (the warp's solves run in lockstep batches of 32) */
 } nrt_wavefront_tuning;
 int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out);
 int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in);
 /* Autotuner: times nrt_intersect (wavefront) on these rays and buffers under
  * candidate launch shapes, one knob at a time (coordinate descent over
- * traversal and scatter grids, class-launch blocks, round quotas and rays
- * per pass; the graph/host-driven choice stays as set), and keeps the
+ * traversal and scatter grids, class-launch blocks, round quotas, the Newton
+ * lane-refill threshold and rays per pass; the graph/host-driven choice stays
+ * as set), and keeps the
  * fastest on the scene.  *out gets it and
  * *best_ms its time per call (CUDA events, `reps` calls after one untimed
  * call).  Synchronous.  Results do not depend on the tuning. */
@@ -282,6 +286,9 @@ typedef struct {
     uint64_t newton_kernel_launches;   /* with kernel timing on: how many such launches */
     uint64_t flat_skips;               /* (ray, patch) tests accepted by flat-skip without Newton
                                           (the reference's skip_count, src/gpu/intersect.cu:111) */
+    uint64_t learned_converged;        /* learned solves that converged from the network's guess */
+    uint64_t learned_fallback_converged; /* learned solves that fell back and then converged in plain
+                                            Newton: with learned_converged, the pairs that have a root */
 } nrt_counters;
 int nrt_enable_counters(nrt_scene* scene, int enable);
 /* Kernel timing for roofline measurement: while enabled, the wavefront runs

@@ -91,7 +91,7 @@ __device__ __forceinline__ bool flat_accept(const float* __restrict__ blk, const
 // Indices into the device counter block (nrt_counters order).
 enum Counter : int {
     kRays = 0, kBoxTests, kCandidates, kCulled, kSolves, kEvals, kFp64Solves, kFp64Final, kHits, kErrors, kLearned,
-    kFallbacks, kRoundsDone, kFlatSkips, kNumCounters
+    kFallbacks, kRoundsDone, kFlatSkips, kLearnedConverged, kFallbackConverged, kNumCounters
 };
 // Followed by 64 per-degree evaluation counts and 64 per-degree hull-test counts.
 constexpr int kEvalsByDegree = kNumCounters, kHullByDegree = kNumCounters + 64, kCounterWords = kNumCounters + 128;

@@ -49,7 +49,9 @@ __device__ __forceinline__ void test_patch(const Scene& sc, int slot, const RayF
             return;
         }
     }
-    const NewtonOut o = newton<P, Q, FINAL>(blk, r, pr, gu, gv, seed, op.nw);
+    NewtonOpts nw = op.nw;  // the FP64 decisions apply to patches with widely spread weights
+    nw.fp64_band = op.nw.fp64_band && ((h.y >> 8) & kFlagWideWeights);
+    const NewtonOut o = newton<P, Q, FINAL>(blk, r, pr, gu, gv, seed, nw);
     ++c.solves;
     c.evals += (unsigned long long)o.done;
     c.f64s += (unsigned long long)o.fp64_solves;

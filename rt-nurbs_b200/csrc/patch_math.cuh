@@ -27,7 +27,11 @@ __device__ __forceinline__ double fmx(double a, double b, double c) { return ::f
 
 // Packed patch header: x = first float of the SoA block, y = p | q<<4 |
 // flags<<8, z = global patch id, w = surface id.
-enum : int { kFlagPositiveWeights = 1 };
+// kFlagWideWeights: the weights span more than kWideWeightRatio (max / min),
+// where the FP32 residual's rounding floor approaches the stop rule's eps and
+// the FP64 decisions of newton_step apply.
+enum : int { kFlagPositiveWeights = 1, kFlagWideWeights = 2 };
+constexpr double kWideWeightRatio = 64.0;
 
 struct RayFrame {
     float ox, oy, oz, dx, dy, dz;
@@ -50,19 +54,19 @@ struct NewtonOpts {
     int fp64_band;   // 1: convergence near eps is decided in FP64 (newton_tail_fp64)
 };
 
-// FP64 decisions of the FP64 final-step mode (op.fp64_band):
+// FP64 decisions of the FP64 final-step mode (op.fp64_band, set per patch for
+// patches flagged kFlagWideWeights):
 //  * the decision band: an FP32 residual in [kBandLo * eps, kBandHi * eps)
 //    hands the solve to FP64, which continues the same iteration from there
 //    (on nets with extreme weights the FP32 residual has a rounding floor near
 //    eps and would stall in this band);
 //  * marginal outcomes: an FP32 solve that converges at one of the last
 //    kLateEvals evaluations of the budget, or that ends unconverged with its
-//    residual below kNearMiss * eps and still falling (below half the one
-//    before), is solved again in FP64 from the same start with the same seeds
-//    and budget, whose outcome stands.  Where the iteration needs the whole
+//    residual below kNearMiss * eps, is solved again in FP64 from the same
+//    start with the same seeds and budget, whose outcome stands.  Where the iteration needs the whole
 //    budget, rounding decides whether it converges in time; these are the
 //    solves on which FP32 and the same method in double part ways.
-constexpr float kBandLo = 0.25f, kBandHi = 2.f, kNearMiss = 4096.f;
+constexpr float kBandLo = 0.125f, kBandHi = 16.f, kNearMiss = 4096.f;
 constexpr int kLateEvals = 2;
 
 struct NewtonOut {
@@ -860,7 +864,7 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
     const bool stuck = !pull && s.u == u && s.v == v;  // a fixed point of the iteration
     if (s.it > op.max_iter || stuck) {
         end();
-        if (!stuck && band && s.res_last < kNearMiss * op.eps && s.res_last < 0.5f * s.res_prev) {
+        if (!stuck && band && s.res_last < kNearMiss * op.eps) {
             resolve_fp64();
             return true;
         }

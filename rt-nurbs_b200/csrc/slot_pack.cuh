@@ -225,10 +225,12 @@ NRT_HD inline void pack_slot(const float* P, int p, int q, const Box3& b, int pa
     const double cx = 0.5 * ((double)b.lo[0] + b.hi[0]), cy = 0.5 * ((double)b.lo[1] + b.hi[1]),
                  cz = 0.5 * ((double)b.lo[2] + b.hi[2]);
     bool pos = true;
-    double rad = 0.0;
+    double rad = 0.0, wmin = INFINITY, wmax = 0.0;
     for (int i = 0; i < n; ++i) {
         const double w = P[4 * i + 3];
         pos = pos && (w > 0.0);
+        wmin = fabs(w) < wmin ? fabs(w) : wmin;
+        wmax = dmax(wmax, fabs(w));
         blk[i] = (float)((double)P[4 * i + 0] - w * cx);
         blk[np + i] = (float)((double)P[4 * i + 1] - w * cy);
         blk[2 * np + i] = (float)((double)P[4 * i + 2] - w * cz);
@@ -242,7 +244,8 @@ NRT_HD inline void pack_slot(const float* P, int p, int q, const Box3& b, int pa
         blk[i] = 0.f; blk[np + i] = 0.f; blk[2 * np + i] = 0.f;
         blk[3 * np + i] = 1.f;
     }
-    hdr = make_int4((int)off, p | (q << 4) | ((pos ? dev::kFlagPositiveWeights : 0) << 8), patch_id, surf);
+    const int flags = (pos ? dev::kFlagPositiveWeights : 0) | (wmax > dev::kWideWeightRatio * wmin ? dev::kFlagWideWeights : 0);
+    hdr = make_int4((int)off, p | (q << 4) | (flags << 8), patch_id, surf);
     ctr = make_double4(cx, cy, cz, rad);
     const int ci[4] = {0, p * (q + 1), p * (q + 1) + q, q};  // q00, q10, q11, q01 (bezier_patch.h:37-44)
     for (int c = 0; c < 4; ++c) {

@@ -40,8 +40,10 @@ __device__ __forceinline__ void item_ray(const WfItem& it, RayFrame& r) {
 template <int P, int Q, bool LEARNED>
 __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const RayFrame& r, const PatchRay& pr,
                                                 const float* __restrict__ blk, float lu, float lv, uint32_t seed,
-                                                const Opts& op, const NewtonOpts& nw, int& fell_back) {
+                                                const Opts& op, const NewtonOpts& nw_in, int& fell_back) {
     fell_back = 0;
+    NewtonOpts nw = nw_in;  // the FP64 decisions apply to patches with widely spread weights
+    nw.fp64_band = nw_in.fp64_band && ((__ldg(&sc.hdr[slot].y) >> 8) & kFlagWideWeights);
     const bool inside = lu >= -0.25f && lu <= 1.25f && lv >= -0.25f && lv <= 1.25f;
     if (LEARNED && inside) {
         NewtonOpts nl = nw;
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
     int* qu = queue[warp];
     const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
     unsigned long long solves = 0, evals = 0, f64 = 0, culled = 0, hull_tests = 0, learned = 0, fallbacks = 0,
-                       flats = 0, cas_err = 0;
+                       flats = 0, cas_err = 0, learned_conv = 0, fallback_conv = 0;
     NewtonOpts nw = op.nw;
     nw.fp64_final = 0;  // applied to the winner only, in k_wf_resolve
     const float cull_eps = op.nw.eps;
@@ -189,6 +191,8 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
             ++solves;
             learned += (kUseNet && fell != 2) ? 1 : 0;
             fallbacks += fell == 1 ? 1ull : 0ull;
+            learned_conv += (kUseNet && fell == 0) ? 1ull : 0ull;      // the guess's own solve converged
+            fallback_conv += (fell == 1 && o.evals > 0) ? 1ull : 0ull;  // it did not, plain Newton did
             evals += (unsigned long long)o.done;
             f64 += (unsigned long long)o.fp64_solves;
             if (tests) atomicAdd(tests + it.ray, 1);
@@ -219,6 +223,8 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
         count_add(ctr, kCulled, culled);
         count_add(ctr, kLearned, learned);
         count_add(ctr, kFallbacks, fallbacks);
+        count_add(ctr, kLearnedConverged, learned_conv);
+        count_add(ctr, kFallbackConverged, fallback_conv);
         count_add(ctr, kFlatSkips, flats);
         if (evals) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, evals);
         if (hull_tests) atomicAdd(ctr + kHullByDegree + P * 8 + Q, hull_tests);
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffer
 #endif
 template <int P, int Q>
 __global__ void __launch_bounds__(256, NRT_NEWTON_MIN_BLOCKS) k_wf_newton_plain(Scene sc, WfBuffers wb, int rank_lo, int rank_hi, Opts op,
-                                                         int32_t* tests, unsigned long long* ctr) {
+                                                         int32_t* tests, unsigned long long* ctr, int refill_min) {
     constexpr unsigned kFull = 0xffffffffu;
     __shared__ int queue[8][64];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -261,11 +267,12 @@ __global__ void __launch_bounds__(256, NRT_NEWTON_MIN_BLOCKS) k_wf_newton_plain(
     RayFrame r;
     PatchRay pr{};
     const float* blk = sc.cp;
+    bool wide = false;
     NewtonState st = newton_start(0.5f, 0.5f, 0u);
     while (true) {
         // idle lanes take queued survivors; the queue is refilled by hull-testing the next chunks
         const unsigned idle = __ballot_sync(kFull, !busy);
-        const int need = __popc(idle);
+        const int need = __popc(idle) >= refill_min ? __popc(idle) : 0;  // refill once enough lanes are idle
         while (more && qn < need) {
             const int base = begin + 32 * chunk;
             chunk += n_warps;
@@ -316,6 +323,7 @@ __global__ void __launch_bounds__(256, NRT_NEWTON_MIN_BLOCKS) k_wf_newton_plain(
                 blk = sc.cp + h.x;
                 ray = it.ray;
                 slot = it.slot;
+                wide = (h.y >> 8) & kFlagWideWeights;
                 ++solves;
                 if (tests) atomicAdd(tests + ray, 1);
                 float gu = 0.5f, gv = 0.5f;
@@ -345,7 +353,9 @@ __global__ void __launch_bounds__(256, NRT_NEWTON_MIN_BLOCKS) k_wf_newton_plain(
         if (!__any_sync(kFull, busy)) break;  // every lane idle after a refill: the input is used up
         if (busy) {
             NewtonOut o;
-            if (newton_step<P, Q, true>(blk, r, pr, st, nw, o)) {
+            NewtonOpts nwl = nw;  // the FP64 decisions apply to patches with widely spread weights
+            nwl.fp64_band = nw.fp64_band && wide;
+            if (newton_step<P, Q, true>(blk, r, pr, st, nwl, o)) {
                 busy = false;
                 evals += (unsigned)o.done;
                 f64 += (unsigned)o.fp64_solves;
@@ -502,8 +512,12 @@ void newton_class(const WfClassLaunch& L) {
                                                                         L.rank_hi, *L.op, L.tests, L.ctr);
             break;
         default:
-            k_wf_newton_plain<P, Q><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op, L.tests,
-                                                                  L.ctr);
+            if (L.refill >= 32)  // lockstep batches of 32 solves
+                k_wf_newton<P, Q, kWfPlain><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.rays, *L.wb, L.cls, L.rank_lo,
+                                                                          L.rank_hi, *L.op, L.tests, L.ctr);
+            else
+                k_wf_newton_plain<P, Q><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op,
+                                                                      L.tests, L.ctr, L.refill);
     }
 }
 

@@ -69,7 +69,9 @@ class Counters(C.Structure):
                                                             ("kernel_launches", C.c_uint64), ("rounds", C.c_uint64),
                                                             ("newton_kernel_ms", C.c_double),
                                                             ("newton_kernel_launches", C.c_uint64),
-                                                            ("flat_skips", C.c_uint64)]
+                                                            ("flat_skips", C.c_uint64),
+                                                            ("learned_converged", C.c_uint64),
+                                                            ("learned_fallback_converged", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: int(getattr(self, k)) for k in _COUNTER_NAMES}
@@ -80,12 +82,15 @@ class Counters(C.Structure):
         d["newton_kernel_ms"] = float(self.newton_kernel_ms)
         d["newton_kernel_launches"] = int(self.newton_kernel_launches)
         d["flat_skips"] = int(self.flat_skips)
+        d["learned_converged"] = int(self.learned_converged)
+        d["learned_fallback_converged"] = int(self.learned_fallback_converged)
         return d
 
 
 class Tuning(C.Structure):
     _fields_ = [("step_blocks", C.c_int64), ("scatter_blocks", C.c_int64), ("class_blocks", C.c_int32),
-                ("graph", C.c_int32), ("chunk", C.c_int64), ("quota0", C.c_int32), ("quota_max", C.c_int32)]
+                ("graph", C.c_int32), ("chunk", C.c_int64), ("quota0", C.c_int32), ("quota_max", C.c_int32),
+                ("newton_refill", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

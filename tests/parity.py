@@ -40,13 +40,25 @@ def compare(gpu, patch_ref, t_ref, u_ref=None, v_ref=None):
     return st
 
 
-def root_stats(oracle_mod, P, rays_np, got, ref):
+def crossing_cos(rays_np, geom):
+    """|cos| of the angle between each ray and the surface normal dS/du x dS/dv
+    of its hit (from the hit's 9-float geometry): t's condition number is about
+    1 / |cos|, so near-tangent crossings (|cos| -> 0) are ill-conditioned."""
+    d = np.stack(rays_np[3:], 1).astype(np.float64)
+    g = geom.astype(np.float64)
+    n = np.cross(g[:, 3:6], g[:, 6:9])
+    return np.abs(np.sum(n * d, 1)) / np.maximum(np.linalg.norm(n, axis=1) * np.linalg.norm(d, axis=1), 1e-300)
+
+
+def root_stats(oracle_mod, P, rays_np, got, ref, cosang=None):
     """Hits of the engine and of the FP64 oracle on the same rays, each refined
     to the exact root next to it (FP64 Newton to |r1|+|r2| < 1e-11 from the
     reported (u, v) on the reported patch; the oracle itself stops at the
     method's eps, so its t is only good to about eps / sin(angle)).  Returns:
     genuine (fraction of engine hits that refine to a root), t_err / uv_err
-    (engine hit against its exact root; max and quantiles), same_root
+    (engine hit against its exact root; max and quantiles; with cosang, the
+    |cos| of each hit's crossing angle, t_err_max is taken over the hits with
+    |cos| >= 1e-2 and t_err_tangent counts the others above 1e-4), same_root
     (fraction of rays both hit where the two exact roots coincide) and the
     counts of rays both hit on different roots, by which one is nearer."""
     rays = oracle_mod.Rays(*rays_np)
@@ -58,9 +70,11 @@ def root_stats(oracle_mod, P, rays_np, got, ref):
     if ok.any():
         rel = np.abs(got["t"][ok].astype(np.float64) - pe.t[ok]) / np.abs(pe.t[ok])
         duv = np.maximum(np.abs(got["u"][ok] - pe.u[ok]), np.abs(got["v"][ok] - pe.v[ok]))
-        st.update({"t_err_max": float(rel.max()), "t_err_p9999": float(np.quantile(rel, 0.9999)),
-                   "t_err_gt_1e-4": int((rel > 1e-4).sum()), "uv_err_max": float(duv.max()),
-                   "uv_err_p999": float(np.quantile(duv, 0.999))})
+        wc = np.ones(rel.size, bool) if cosang is None else cosang[ok] >= 1e-2
+        st.update({"t_err_max": float(rel[wc].max()) if wc.any() else 0.0,
+                   "t_err_max_all": float(rel.max()), "t_err_p9999": float(np.quantile(rel, 0.9999)),
+                   "t_err_gt_1e-4": int((rel > 1e-4).sum()), "t_err_tangent": int(((rel > 1e-4) & ~wc).sum()),
+                   "uv_err_max": float(duv.max()), "uv_err_p999": float(np.quantile(duv, 0.999))})
     both = he & ho & (pe.patch >= 0) & (po.patch >= 0)
     same = both & (got["patch"] == ref.patch) & (np.abs(pe.t - po.t) <= 1e-6 * np.abs(po.t))
     st["same_root"] = float(same.sum() / max(both.sum(), 1))
