@@ -761,6 +761,8 @@ struct NewtonState {
     int it;      // the evaluation about to run, 1-based
     int done;    // evaluations run
     int f64;     // 2x2 steps solved in FP64 so far
+    int fp64;    // how the solve ended: 0 decided in FP32, 1 FP64 continues from (u, v) at
+                 // evaluation it, 2 solved again in FP64 from the start (newton_finish)
 };
 
 __device__ __forceinline__ NewtonState newton_start(float u0, float v0, uint32_t seed) {
@@ -771,11 +773,14 @@ __device__ __forceinline__ NewtonState newton_start(float u0, float v0, uint32_t
     s.it = 1;
     s.done = 0;
     s.f64 = 0;
+    s.fp64 = 0;
     return s;
 }
 
 // One evaluation (and step) of the solve in s.  Returns true when the solve
-// has ended, with o holding its outcome (o is written only then).
+// has ended, with o holding its FP32 outcome (o is written only then); the
+// FP64 work that decides or refines it is left to newton_finish, so that the
+// evaluation loop makes no calls.
 template <int P, int Q, bool FINAL = true>
 __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
                                             NewtonState& s, const NewtonOpts& op, NewtonOut& o) {
@@ -793,11 +798,6 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
         o.u = s.u; o.v = s.v;
         return true;
     }
-    // the whole solve again in FP64, from the same start with the same seeds
-    auto resolve_fp64 = [&]() {
-        newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, s.u0, s.v0, 1, s.seed0, op, o);
-        if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
-    };
     const float u = s.u, v = s.v;
     float H[4], Hu[4], Hv[4];
     eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
@@ -813,13 +813,12 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
     s.res_last = res;
     if (band && res >= accept && res < kBandHi * op.eps) {
         end();
-        newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, u, v, s.it, s.seed, op, o);
-        if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
+        s.fp64 = 1;  // FP64 continues from (u, v) at this evaluation
         return true;
     }
     if (band && res < accept && s.it > op.max_iter - kLateEvals) {
         end();
-        resolve_fp64();
+        s.fp64 = 2;  // a late convergence: the whole solve again in FP64
         return true;
     }
     if (res < accept) {
@@ -830,7 +829,6 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
         o.ux = ux; o.uy = uy; o.uz = uz;
         o.vx = vx; o.vy = vy; o.vz = vz;
         o.t = fmaf(sx, r.dx, fmaf(sy, r.dy, fmaf(sz, r.dz, pr.tc)));
-        if (FINAL && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
         return true;
     }
     const float j11 = r.n1x * ux + r.n1y * uy + r.n1z * uz;
@@ -864,15 +862,23 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
     const bool stuck = !pull && s.u == u && s.v == v;  // a fixed point of the iteration
     if (s.it > op.max_iter || stuck) {
         end();
-        if (!stuck && band && s.res_last < kNearMiss * op.eps) {
-            resolve_fp64();
-            return true;
-        }
         o.evals = -op.max_iter;
         o.u = s.u; o.v = s.v;
+        if (!stuck && band && s.res_last < kNearMiss * op.eps) s.fp64 = 2;  // a near miss: again in FP64
         return true;
     }
     return false;
+}
+
+// The FP64 part of an ended solve: the continuation or the whole solve in
+// FP64 that newton_step asked for, then, when converged and op.fp64_final, the
+// FP64 refinement of the point.
+template <int P, int Q>
+__device__ __forceinline__ void newton_finish(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
+                                              const NewtonState& s, const NewtonOpts& op, NewtonOut& o) {
+    if (s.fp64 == 1) newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, s.u, s.v, s.it, s.seed, op, o);
+    else if (s.fp64 == 2) newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, s.u0, s.v0, 1, s.seed0, op, o);
+    if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
 }
 
 template <int P, int Q, bool FINAL = true>
@@ -882,6 +888,7 @@ __device__ __forceinline__ NewtonOut newton(const float* __restrict__ blk, const
     NewtonState s = newton_start(u0, v0, seed);
     while (!newton_step<P, Q, FINAL>(blk, r, pr, s, op, o)) {
     }
+    if (FINAL) newton_finish<P, Q>(blk, r, pr, s, op, o);
     return o;
 }
 

@@ -101,7 +101,7 @@ __device__ __forceinline__ void item_features(const Scene& sc, bool valid, int s
 // and queues the survivors in shared memory; Newton then runs on full warps of
 // survivors, so culled items do not leave lanes idle.
 template <int P, int Q, int MODE>
-__global__ void __launch_bounds__(256) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
+__global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
                                                    int rank_hi, Opts op, int32_t* tests, unsigned long long* ctr) {
     constexpr unsigned kFull = 0xffffffffu;
     constexpr bool kUseNet = MODE == kWfLearned, kFeatures = MODE != kWfPlain;
@@ -356,6 +356,7 @@ __global__ void __launch_bounds__(256, NRT_NEWTON_MIN_BLOCKS) k_wf_newton_plain(
             NewtonOpts nwl = nw;  // the FP64 decisions apply to patches with widely spread weights
             nwl.fp64_band = nw.fp64_band && wide;
             if (newton_step<P, Q, true>(blk, r, pr, st, nwl, o)) {
+                newton_finish<P, Q>(blk, r, pr, st, nwl, o);
                 busy = false;
                 evals += (unsigned)o.done;
                 f64 += (unsigned)o.fp64_solves;
