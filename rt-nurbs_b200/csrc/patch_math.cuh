@@ -54,20 +54,13 @@ struct NewtonOpts {
     int fp64_band;   // 1: convergence near eps is decided in FP64 (newton_tail_fp64)
 };
 
-// FP64 decisions of the FP64 final-step mode (op.fp64_band, set per patch for
-// patches flagged kFlagWideWeights):
-//  * the decision band: an FP32 residual in [kBandLo * eps, kBandHi * eps)
-//    hands the solve to FP64, which continues the same iteration from there
-//    (on nets with extreme weights the FP32 residual has a rounding floor near
-//    eps and would stall in this band);
-//  * marginal outcomes: an FP32 solve that converges at one of the last
-//    kLateEvals evaluations of the budget, or that ends unconverged with its
-//    residual below kNearMiss * eps, is solved again in FP64 from the same
-//    start with the same seeds and budget, whose outcome stands.  Where the iteration needs the whole
-//    budget, rounding decides whether it converges in time; these are the
-//    solves on which FP32 and the same method in double part ways.
-constexpr float kBandLo = 0.125f, kBandHi = 16.f, kNearMiss = 4096.f;
-constexpr int kLateEvals = 2;
+// The FP64 decision band of the FP64 final-step mode (op.fp64_band, set per
+// patch for patches flagged kFlagWideWeights): an FP32 residual below
+// kBandLo * eps is accepted as converged, and one in [kBandLo * eps,
+// kBandHi * eps) hands the solve to FP64, which continues the same iteration
+// from there with the evaluations left (on nets with extreme weights the FP32
+// residual has a rounding floor near eps and would stall in this band).
+constexpr float kBandLo = 0.125f, kBandHi = 16.f;
 
 struct NewtonOut {
     int evals;       // > 0 converged after this many evaluations; < 0 not converged
@@ -741,8 +734,7 @@ __device__ __noinline__ void newton_tail_fp64(const float* __restrict__ blk, con
 // cond_fp64 > 0 and ||J||_F^2 / |det J| exceeds it, the 2x2 solve is done in
 // FP64 (products of floats are exact there, so det J has no cancellation).
 // With op.fp64_band (the FP64 final-step mode) convergence within the
-// decision band around eps, and the marginal outcomes, are decided in FP64
-// (newton_tail_fp64).  FINAL = false compiles the FP64 final step and the FP64
+// decision band around eps is decided in FP64 (newton_tail_fp64).  FINAL = false compiles the FP64 final step and the FP64
 // decisions out (for kernels that run without them, so that they carry no
 // call to them).
 //
@@ -756,20 +748,18 @@ __device__ __noinline__ void newton_tail_fp64(const float* __restrict__ blk, con
 // the evaluations actually run; the outcome, -max_iter, is unchanged).
 struct NewtonState {
     float u, v, u0, v0;
-    float res_prev, res_last;
-    uint32_t seed, seed0;
+    uint32_t seed;
     int it;      // the evaluation about to run, 1-based
     int done;    // evaluations run
     int f64;     // 2x2 steps solved in FP64 so far
-    int fp64;    // how the solve ended: 0 decided in FP32, 1 FP64 continues from (u, v) at
-                 // evaluation it, 2 solved again in FP64 from the start (newton_finish)
+    int fp64;    // 1: the solve ended in the decision band; FP64 continues from (u, v) at
+                 // evaluation it (newton_finish)
 };
 
 __device__ __forceinline__ NewtonState newton_start(float u0, float v0, uint32_t seed) {
     NewtonState s;
     s.u = u0; s.v = v0; s.u0 = u0; s.v0 = v0;
-    s.res_prev = INFINITY; s.res_last = INFINITY;
-    s.seed = seed; s.seed0 = seed;
+    s.seed = seed;
     s.it = 1;
     s.done = 0;
     s.f64 = 0;
@@ -809,16 +799,9 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
     const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));
     const float r2 = fmaf(r.n2x, sx, fmaf(r.n2y, sy, fmaf(r.n2z, sz, pr.e2)));
     const float res = fabsf(r1) + fabsf(r2);
-    s.res_prev = s.res_last;
-    s.res_last = res;
     if (band && res >= accept && res < kBandHi * op.eps) {
         end();
         s.fp64 = 1;  // FP64 continues from (u, v) at this evaluation
-        return true;
-    }
-    if (band && res < accept && s.it > op.max_iter - kLateEvals) {
-        end();
-        s.fp64 = 2;  // a late convergence: the whole solve again in FP64
         return true;
     }
     if (res < accept) {
@@ -864,20 +847,17 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
         end();
         o.evals = -op.max_iter;
         o.u = s.u; o.v = s.v;
-        if (!stuck && band && s.res_last < kNearMiss * op.eps) s.fp64 = 2;  // a near miss: again in FP64
         return true;
     }
     return false;
 }
 
-// The FP64 part of an ended solve: the continuation or the whole solve in
-// FP64 that newton_step asked for, then, when converged and op.fp64_final, the
-// FP64 refinement of the point.
+// The FP64 part of an ended solve: the FP64 continuation newton_step asked
+// for, then, when converged and op.fp64_final, the FP64 refinement of the point.
 template <int P, int Q>
 __device__ __forceinline__ void newton_finish(const float* __restrict__ blk, const RayFrame& r, const PatchRay& pr,
                                               const NewtonState& s, const NewtonOpts& op, NewtonOut& o) {
     if (s.fp64 == 1) newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, s.u, s.v, s.it, s.seed, op, o);
-    else if (s.fp64 == 2) newton_tail_fp64<P, Q>(blk, r, pr, s.u0, s.v0, s.u0, s.v0, 1, s.seed0, op, o);
     if (o.evals > 0 && op.fp64_final) final_step_fp64<P, Q>(blk, r, pr, o);
 }
 
