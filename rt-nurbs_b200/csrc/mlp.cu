@@ -1,6 +1,8 @@
 // mlp.cu -- training and inference entry points of the learned-initial-guess
-// MLP (12 -> 64 -> 64 -> 2, SiLU), all on BF16 tensor cores (mma.sync
-// m16n8k16, FP32 accumulation) with FP32 master weights and Adam.
+// MLP (12 -> 64 -> 64 -> 2, SiLU) with FP32 master weights and Adam.
+// Training forward + backward runs on the tcgen05 tensor cores (mlp_tc.cu,
+// FP32 accumulators in tensor memory); inference on BF16 mma.sync m16n8k16
+// (mlp.cuh), FP32 accumulation.
 //
 // Rounding points (mirrored by the CPU oracle, oracle/mlp_oracle.py): every
 // tensor-core operand is bfloat16 (inputs, weights, hidden activations, output
@@ -99,318 +101,6 @@ __global__ void k_mlp_adam(float* master, float* m, float* v, float* grad, char*
     master[k] = w;
     grad[k] = 0.f;
     put_blob(blob, k, w);
-}
-
-struct TrainWarp {
-    __nv_bfloat16 x[32][kMlpLdIn];
-    __nv_bfloat16 h1[32][kMlpLd], h2[32][kMlpLd], dz[32][kMlpLd];
-    __nv_bfloat16 dy[32][kMlpLdIn];
-    float z1[32][64], z2[32][64];
-    float t[32][2];
-};
-
-struct TrainSmem {
-    __nv_bfloat16 w1t[64][kMlpLdIn], w2t[64][kMlpLd], w3t[8][kMlpLd];
-    float b1[64], b2[64], b3[8];
-    float gw1[64][16], gb1[64], gw2[64][64], gb2[64], gw3[8][64], gb3[8];
-    float loss;
-    TrainWarp w[4];
-};
-
-__device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
-
-// Sum a value over the 8 lanes that share threadIdx & 3 (the rows of a fragment column).
-__device__ __forceinline__ float sum_over_rows(float x) {
-    x += __shfl_xor_sync(0xffffffffu, x, 4);
-    x += __shfl_xor_sync(0xffffffffu, x, 8);
-    x += __shfl_xor_sync(0xffffffffu, x, 16);
-    return x;
-}
-
-// Forward + backward over `count` samples starting at `begin` (through perm if
-// given); weight and bias gradients of mean((Y-T)^2) summed into grad (public
-// order), the batch loss into *loss.  Blocks of 4 warps, 32 samples per warp.
-__global__ void __launch_bounds__(128) k_mlp_fwd_bwd(MlpParams P, const float* __restrict__ X,
-                                                     const float* __restrict__ T, const int32_t* __restrict__ perm,
-                                                     long long begin, long long count, float inv_batch, float* grad,
-                                                     float* loss) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
-    for (int k = threadIdx.x; k < 64 * 16; k += blockDim.x) s.w1t[k / 16][k % 16] = P.w1t[k];
-    for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) s.w2t[k / 64][k % 64] = P.w2t[k];
-    for (int k = threadIdx.x; k < 8 * 64; k += blockDim.x) s.w3t[k / 64][k % 64] = P.w3t[k];
-    for (int k = threadIdx.x; k < 64; k += blockDim.x) {
-        s.b1[k] = P.b1[k];
-        s.b2[k] = P.b2[k];
-        s.gb1[k] = 0.f;
-        s.gb2[k] = 0.f;
-    }
-    for (int k = threadIdx.x; k < 8; k += blockDim.x) {
-        s.b3[k] = P.b3[k];
-        s.gb3[k] = 0.f;
-    }
-    for (int k = threadIdx.x; k < 64 * 16; k += blockDim.x) (&s.gw1[0][0])[k] = 0.f;
-    for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) (&s.gw2[0][0])[k] = 0.f;
-    for (int k = threadIdx.x; k < 8 * 64; k += blockDim.x) (&s.gw3[0][0])[k] = 0.f;
-    if (threadIdx.x == 0) s.loss = 0.f;
-    __syncthreads();
-    TrainWarp& W = s.w[warp];
-    const long long tiles = (count + 31) / 32;
-    float my_loss = 0.f;
-    for (long long tile = (long long)blockIdx.x * 4 + warp; tile < tiles; tile += (long long)gridDim.x * 4) {
-        const long long row = tile * 32 + lane;
-        const bool valid = row < count;
-        const long long smp = valid ? (perm ? (long long)perm[begin + row] : begin + row) : 0;
-#pragma unroll
-        for (int k = 0; k < 16; k += 2) {
-            const float a = (valid && k < 12) ? X[smp * 12 + k] : 0.f;
-            const float b = (valid && k + 1 < 12) ? X[smp * 12 + k + 1] : 0.f;
-            *reinterpret_cast<uint32_t*>(&W.x[lane][k]) = pack_bf16(a, b);
-        }
-        W.t[lane][0] = valid ? T[smp * 2] : 0.f;
-        W.t[lane][1] = valid ? T[smp * 2 + 1] : 0.f;
-        for (int k = 0; k < 16; ++k) W.dy[lane][k] = __float2bfloat16_rn(0.f);
-        __syncwarp();
-        // ---- forward: layer 1 (K = 16) and layer 2 (K = 64), keeping the pre-activations
-#pragma unroll
-        for (int layer = 0; layer < 2; ++layer) {
-            float acc[2][8][4];
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                for (int nt = 0; nt < 8; ++nt) {
-                    acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.f;
-                    const int ksteps = layer == 0 ? 1 : 4;
-                    for (int ks = 0; ks < ksteps; ++ks) {
-                        const int r0 = mt * 16, c0 = ks * 16;
-                        uint32_t a0, a1, a2, a3, b0, b1;
-                        if (layer == 0) {
-                            a0 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][c0 + 2 * t4]);
-                            a1 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][c0 + 2 * t4]);
-                            a2 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][c0 + 2 * t4 + 8]);
-                            a3 = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][c0 + 2 * t4 + 8]);
-                            b0 = *reinterpret_cast<const uint32_t*>(&s.w1t[nt * 8 + g][c0 + 2 * t4]);
-                            b1 = *reinterpret_cast<const uint32_t*>(&s.w1t[nt * 8 + g][c0 + 2 * t4 + 8]);
-                        } else {
-                            a0 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g][c0 + 2 * t4]);
-                            a1 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g + 8][c0 + 2 * t4]);
-                            a2 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g][c0 + 2 * t4 + 8]);
-                            a3 = *reinterpret_cast<const uint32_t*>(&W.h1[r0 + g + 8][c0 + 2 * t4 + 8]);
-                            b0 = *reinterpret_cast<const uint32_t*>(&s.w2t[nt * 8 + g][c0 + 2 * t4]);
-                            b1 = *reinterpret_cast<const uint32_t*>(&s.w2t[nt * 8 + g][c0 + 2 * t4 + 8]);
-                        }
-                        mma_bf16(acc[mt][nt], a0, a1, a2, a3, b0, b1);
-                    }
-                }
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                for (int nt = 0; nt < 8; ++nt) {
-                    const int col = nt * 8 + 2 * t4, r = mt * 16 + g;
-                    const float* bias = layer == 0 ? s.b1 : s.b2;
-                    float(*z)[64] = layer == 0 ? W.z1 : W.z2;
-                    __nv_bfloat16(*h)[kMlpLd] = layer == 0 ? W.h1 : W.h2;
-                    const float v0 = acc[mt][nt][0] + bias[col], v1 = acc[mt][nt][1] + bias[col + 1];
-                    const float v2 = acc[mt][nt][2] + bias[col], v3 = acc[mt][nt][3] + bias[col + 1];
-                    z[r][col] = v0; z[r][col + 1] = v1; z[r + 8][col] = v2; z[r + 8][col + 1] = v3;
-                    *reinterpret_cast<uint32_t*>(&h[r][col]) = pack_bf16(silu(v0), silu(v1));
-                    *reinterpret_cast<uint32_t*>(&h[r + 8][col]) = pack_bf16(silu(v2), silu(v3));
-                }
-            __syncwarp();
-        }
-        // ---- output layer and dY = 2 (Y - T) / B
-        {
-            float gb3_0 = 0.f, gb3_1 = 0.f;
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int ks = 0; ks < 4; ++ks) {
-                    const int r0 = mt * 16, c0 = ks * 16;
-                    mma_bf16(d, *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g][c0 + 2 * t4]),
-                             *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g + 8][c0 + 2 * t4]),
-                             *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g][c0 + 2 * t4 + 8]),
-                             *reinterpret_cast<const uint32_t*>(&W.h2[r0 + g + 8][c0 + 2 * t4 + 8]),
-                             *reinterpret_cast<const uint32_t*>(&s.w3t[g][c0 + 2 * t4]),
-                             *reinterpret_cast<const uint32_t*>(&s.w3t[g][c0 + 2 * t4 + 8]));
-                }
-                if (t4 == 0) {  // columns 0 and 1 are the real outputs
-                    const int r = mt * 16 + g;
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int rr = r + 8 * h;
-                        const bool ok = tile * 32 + rr < count;
-                        const float y0 = d[2 * h] + s.b3[0], y1 = d[2 * h + 1] + s.b3[1];
-                        const float e0 = ok ? y0 - W.t[rr][0] : 0.f, e1 = ok ? y1 - W.t[rr][1] : 0.f;
-                        my_loss += e0 * e0 + e1 * e1;
-                        const float d0 = 2.f * e0 * inv_batch, d1 = 2.f * e1 * inv_batch;
-                        gb3_0 += d0;
-                        gb3_1 += d1;
-                        *reinterpret_cast<uint32_t*>(&W.dy[rr][0]) = pack_bf16(d0, d1);
-                    }
-                }
-            }
-            gb3_0 = sum_over_rows(gb3_0);
-            gb3_1 = sum_over_rows(gb3_1);
-            if (lane == 0) {
-                atomicAdd(&s.gb3[0], gb3_0);
-                atomicAdd(&s.gb3[1], gb3_1);
-            }
-        }
-        __syncwarp();
-        // ---- dW3 = dY^T H2  (M = outputs 0..15, N = 64, K = 32 rows)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
-                const int k0 = ks * 16 + 2 * t4;
-                const uint32_t a0 = pack_bf16(bf(W.dy[k0][g]), bf(W.dy[k0 + 1][g]));
-                const uint32_t a1 = pack_bf16(bf(W.dy[k0][g + 8]), bf(W.dy[k0 + 1][g + 8]));
-                const uint32_t a2 = pack_bf16(bf(W.dy[k0 + 8][g]), bf(W.dy[k0 + 9][g]));
-                const uint32_t a3 = pack_bf16(bf(W.dy[k0 + 8][g + 8]), bf(W.dy[k0 + 9][g + 8]));
-                const uint32_t b0 = pack_bf16(bf(W.h2[k0][nt * 8 + g]), bf(W.h2[k0 + 1][nt * 8 + g]));
-                const uint32_t b1 = pack_bf16(bf(W.h2[k0 + 8][nt * 8 + g]), bf(W.h2[k0 + 9][nt * 8 + g]));
-                mma_bf16(d, a0, a1, a2, a3, b0, b1);
-            }
-            if (g < 8) {
-                atomicAdd(&s.gw3[g][nt * 8 + 2 * t4], d[0]);
-                atomicAdd(&s.gw3[g][nt * 8 + 2 * t4 + 1], d[1]);
-            }
-        }
-        // ---- dH2 = dY W3, dZ2 = dH2 * silu'(Z2)
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-                const int r0 = mt * 16;
-                const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g][2 * t4]);
-                const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g + 8][2 * t4]);
-                const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g][2 * t4 + 8]);
-                const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&W.dy[r0 + g + 8][2 * t4 + 8]);
-                const uint32_t b0 = pack_bf16(bf(s.w3t[2 * t4][nt * 8 + g]), bf(s.w3t[2 * t4 + 1][nt * 8 + g]));
-                const uint32_t b1 = 0u;  // output rows 8..15 do not exist
-                mma_bf16(d, a0, a1, a2, a3, b0, b1);
-                const int col = nt * 8 + 2 * t4, r = r0 + g;
-                float dz[4];
-                dz[0] = d[0] * dsilu_f(W.z2[r][col]);
-                dz[1] = d[1] * dsilu_f(W.z2[r][col + 1]);
-                dz[2] = d[2] * dsilu_f(W.z2[r + 8][col]);
-                dz[3] = d[3] * dsilu_f(W.z2[r + 8][col + 1]);
-                *reinterpret_cast<uint32_t*>(&W.dz[r][col]) = pack_bf16(dz[0], dz[1]);
-                *reinterpret_cast<uint32_t*>(&W.dz[r + 8][col]) = pack_bf16(dz[2], dz[3]);
-                const float c0 = sum_over_rows(dz[0] + dz[2]), c1 = sum_over_rows(dz[1] + dz[3]);
-                if (g == 0) {
-                    atomicAdd(&s.gb2[col], c0);
-                    atomicAdd(&s.gb2[col + 1], c1);
-                }
-            }
-        __syncwarp();
-        // ---- dW2 = dZ2^T H1 (M = 64, N = 64, K = 32 rows)
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                    const int k0 = ks * 16 + 2 * t4, m0 = mt * 16 + g, n0 = nt * 8 + g;
-                    const uint32_t a0 = pack_bf16(bf(W.dz[k0][m0]), bf(W.dz[k0 + 1][m0]));
-                    const uint32_t a1 = pack_bf16(bf(W.dz[k0][m0 + 8]), bf(W.dz[k0 + 1][m0 + 8]));
-                    const uint32_t a2 = pack_bf16(bf(W.dz[k0 + 8][m0]), bf(W.dz[k0 + 9][m0]));
-                    const uint32_t a3 = pack_bf16(bf(W.dz[k0 + 8][m0 + 8]), bf(W.dz[k0 + 9][m0 + 8]));
-                    const uint32_t b0 = pack_bf16(bf(W.h1[k0][n0]), bf(W.h1[k0 + 1][n0]));
-                    const uint32_t b1 = pack_bf16(bf(W.h1[k0 + 8][n0]), bf(W.h1[k0 + 9][n0]));
-                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
-                }
-                const int m = mt * 16 + g, n = nt * 8 + 2 * t4;
-                atomicAdd(&s.gw2[m][n], d[0]);
-                atomicAdd(&s.gw2[m][n + 1], d[1]);
-                atomicAdd(&s.gw2[m + 8][n], d[2]);
-                atomicAdd(&s.gw2[m + 8][n + 1], d[3]);
-            }
-        // ---- dH1 = dZ2 W2, then dZ1 = dH1 * silu'(Z1) (overwrites dz after all reads)
-        float dh1[2][8][4];
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                dh1[mt][nt][0] = dh1[mt][nt][1] = dh1[mt][nt][2] = dh1[mt][nt][3] = 0.f;
-#pragma unroll
-                for (int ks = 0; ks < 4; ++ks) {
-                    const int r0 = mt * 16, c0 = ks * 16, k0 = c0 + 2 * t4, n0 = nt * 8 + g;
-                    const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g][k0]);
-                    const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g + 8][k0]);
-                    const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g][k0 + 8]);
-                    const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&W.dz[r0 + g + 8][k0 + 8]);
-                    const uint32_t b0 = pack_bf16(bf(s.w2t[k0][n0]), bf(s.w2t[k0 + 1][n0]));
-                    const uint32_t b1 = pack_bf16(bf(s.w2t[k0 + 8][n0]), bf(s.w2t[k0 + 9][n0]));
-                    mma_bf16(dh1[mt][nt], a0, a1, a2, a3, b0, b1);
-                }
-            }
-        __syncwarp();
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                const int col = nt * 8 + 2 * t4, r = mt * 16 + g;
-                float dz[4];
-                dz[0] = dh1[mt][nt][0] * dsilu_f(W.z1[r][col]);
-                dz[1] = dh1[mt][nt][1] * dsilu_f(W.z1[r][col + 1]);
-                dz[2] = dh1[mt][nt][2] * dsilu_f(W.z1[r + 8][col]);
-                dz[3] = dh1[mt][nt][3] * dsilu_f(W.z1[r + 8][col + 1]);
-                *reinterpret_cast<uint32_t*>(&W.dz[r][col]) = pack_bf16(dz[0], dz[1]);
-                *reinterpret_cast<uint32_t*>(&W.dz[r + 8][col]) = pack_bf16(dz[2], dz[3]);
-                const float c0 = sum_over_rows(dz[0] + dz[2]), c1 = sum_over_rows(dz[1] + dz[3]);
-                if (g == 0) {
-                    atomicAdd(&s.gb1[col], c0);
-                    atomicAdd(&s.gb1[col + 1], c1);
-                }
-            }
-        __syncwarp();
-        // ---- dW1 = dZ1^T X (M = 64, N = 16, K = 32 rows)
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                    const int k0 = ks * 16 + 2 * t4, m0 = mt * 16 + g, n0 = nt * 8 + g;
-                    const uint32_t a0 = pack_bf16(bf(W.dz[k0][m0]), bf(W.dz[k0 + 1][m0]));
-                    const uint32_t a1 = pack_bf16(bf(W.dz[k0][m0 + 8]), bf(W.dz[k0 + 1][m0 + 8]));
-                    const uint32_t a2 = pack_bf16(bf(W.dz[k0 + 8][m0]), bf(W.dz[k0 + 9][m0]));
-                    const uint32_t a3 = pack_bf16(bf(W.dz[k0 + 8][m0 + 8]), bf(W.dz[k0 + 9][m0 + 8]));
-                    const uint32_t b0 = pack_bf16(bf(W.x[k0][n0]), bf(W.x[k0 + 1][n0]));
-                    const uint32_t b1 = pack_bf16(bf(W.x[k0 + 8][n0]), bf(W.x[k0 + 9][n0]));
-                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
-                }
-                const int m = mt * 16 + g, n = nt * 8 + 2 * t4;
-                atomicAdd(&s.gw1[m][n], d[0]);
-                atomicAdd(&s.gw1[m][n + 1], d[1]);
-                atomicAdd(&s.gw1[m + 8][n], d[2]);
-                atomicAdd(&s.gw1[m + 8][n + 1], d[3]);
-            }
-        __syncwarp();
-    }
-    my_loss = sum_over_rows(my_loss);
-    my_loss += __shfl_xor_sync(0xffffffffu, my_loss, 1);
-    my_loss += __shfl_xor_sync(0xffffffffu, my_loss, 2);
-    if (lane == 0) atomicAdd(&s.loss, my_loss);
-    __syncthreads();
-    for (int k = threadIdx.x; k < kNumParams; k += blockDim.x) {
-        float v;
-        if (k < kP_B1) v = s.gw1[k / 12][k % 12];
-        else if (k < kP_W2) v = s.gb1[k - kP_B1];
-        else if (k < kP_B2) v = (&s.gw2[0][0])[k - kP_W2];
-        else if (k < kP_W3) v = s.gb2[k - kP_B2];
-        else if (k < kP_B3) v = (&s.gw3[0][0])[k - kP_W3];
-        else v = s.gb3[k - kP_B3];
-        if (v != 0.f) atomicAdd(grad + k, v);
-    }
-    if (threadIdx.x == 0) atomicAdd(loss, s.loss * inv_batch);
 }
 
 // Inference on feature rows (n x 12) -> outputs (n x 2), unclamped.

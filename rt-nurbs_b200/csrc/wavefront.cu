@@ -436,7 +436,7 @@ static void wf_resolve_class(int p, int q, const WfClassLaunch& L) {
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds, cudaEvent_t* ev,
-                             double* newton_ms, long long* newton_launches, int quota0, int quota_max, int refill) {
+                             double* newton_ms, long long* newton_launches, int quota0, int quota_max) {
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     int n_active = (int)n, cur = 0;
@@ -444,7 +444,6 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
     L.sc = &sc; L.rays = &rays; L.wb = &wb; L.op = &op; L.out = &out;
     L.tests = out.tests; L.ctr = ctr; L.stream = stream;
     L.mode = op.init_mode == 2 ? kWfLearned : (op.col_feat ? kWfCollect : kWfPlain);
-    L.refill = refill;
     for (int round = 0; n_active > 0; ++round) {
         if (round > 4096) return cudaErrorUnknown;  // unreachable: every round pops at least one entry per ray
         e = cudaMemsetAsync(wb.hist, 0, sizeof(int) * plan.n_slots, stream);
@@ -569,7 +568,7 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
         oc.seed_offset = op.seed_offset + (uint32_t)at;  // seeds follow the global ray index
         WfClassLaunch L{};
         L.sc = &sc; L.rays = &rc; L.wb = &wb; L.op = &oc; L.out = &hc;
-        L.tests = hc.tests; L.ctr = ctr; L.stream = cs; L.mode = mode; L.refill = tu.refill;
+        L.tests = hc.tests; L.ctr = ctr; L.stream = cs; L.mode = mode;
         // the pass's set-up
         cudaGraph_t pre = nullptr;
         e = capture(cs, &pre, [&] {

@@ -75,7 +75,6 @@ struct WfClassLaunch {
     int mode;
     int cls, rank_lo, rank_hi;
     unsigned grid;
-    int refill;    // plain mode: refill threshold (32: the lockstep kernel)
 };
 
 // Launchers of the per-class kernels for u-degree p (wf_solve.cu, one object
@@ -107,7 +106,6 @@ struct WfTuning {
     int class_blocks = 0;               // k_wf_newton blocks of 256 per class launch; 0 = the plan's
     int quota0 = 4;                     // candidates per ray in the first round (doubling each round)
     int quota_max = 8;                  // ... up to this many (<= 8)
-    int refill = 32;                    // plain Newton: idle lanes of a warp before it refills them (32: lockstep)
 };
 
 // The whole intersection of n rays as one executable CUDA graph, in passes of
@@ -130,7 +128,7 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds,
                              cudaEvent_t* ev = nullptr, double* newton_ms = nullptr, long long* newton_launches = nullptr,
-                             int quota0 = 1, int quota_max = 8, int refill = 32);
+                             int quota0 = 1, int quota_max = 8);
 
 // Per-pixel kernel over a device list of ray indices (count read on the device).
 cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const int32_t* list,
@@ -145,7 +143,7 @@ struct NoallocViews {
     dev::Opts opts;
     unsigned long long* counters;
     int device;
-    int quota0, quota_max, refill;
+    int quota0, quota_max;
 };
 
 }  // namespace nrt

@@ -232,155 +232,6 @@ __global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuf
     if (ctr && cas_err) atomicAdd(ctr + kErrors, cas_err);
 }
 
-// The plain solve over the items of one degree class, with per-lane refill.
-// As k_wf_newton, each warp takes 32-item chunks in a fixed stride, runs the
-// hull tests one lane per item and queues the survivors in shared memory.
-// Newton then advances one evaluation at a time on every lane (newton_step),
-// and a lane whose solve has ended takes the next queued survivor at once, so
-// lanes do not wait for the slowest solve of their batch (solves from the
-// midpoint end after anything from 1 to max_iter evaluations).  The closest
-// hit per ray is a minimum over all candidates, so the order in which solves
-// end changes nothing.
-#ifndef NRT_NEWTON_MIN_BLOCKS
-#define NRT_NEWTON_MIN_BLOCKS 1  // blocks of 256 per SM the register allocation must allow
-#endif
-template <int P, int Q>
-__global__ void __launch_bounds__(256, NRT_NEWTON_MIN_BLOCKS) k_wf_newton_plain(Scene sc, WfBuffers wb, int rank_lo, int rank_hi, Opts op,
-                                                         int32_t* tests, unsigned long long* ctr, int refill_min) {
-    constexpr unsigned kFull = 0xffffffffu;
-    __shared__ int queue[8][64];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* qu = queue[warp];
-    const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
-    unsigned solves = 0, evals = 0, f64 = 0, culled = 0, hull_tests = 0, flats = 0, cas_err = 0;  // per thread
-    NewtonOpts nw = op.nw;
-    nw.fp64_final = 0;  // applied to the winner only, in k_wf_resolve
-    const float cull_eps = op.nw.eps;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    int qn = 0;
-    bool more = true;
-    const int n_warps = gridDim.x * (blockDim.x >> 5);
-    int chunk = blockIdx.x * (blockDim.x >> 5) + warp;
-    // the lane's solve in progress
-    bool busy = false;
-    int ray = 0, slot = 0;
-    RayFrame r;
-    PatchRay pr{};
-    const float* blk = sc.cp;
-    bool wide = false;
-    NewtonState st = newton_start(0.5f, 0.5f, 0u);
-    while (true) {
-        // idle lanes take queued survivors; the queue is refilled by hull-testing the next chunks
-        const unsigned idle = __ballot_sync(kFull, !busy);
-        const int need = __popc(idle) >= refill_min ? __popc(idle) : 0;  // refill once enough lanes are idle
-        while (more && qn < need) {
-            const int base = begin + 32 * chunk;
-            chunk += n_warps;
-            if (base >= end) {
-                more = false;
-                break;
-            }
-            const int k = base + lane;
-            bool keep = false;
-            if (k < end) {
-                keep = true;
-                if (op.hull_cull) {
-                    const WfItem it = wb.items[k];
-                    const int4 h = sc.hdr[it.slot];
-                    if ((h.y >> 8) & kFlagPositiveWeights) {
-                        RayFrame rr;
-                        item_ray(it, rr);
-                        const double4 C = sc.centre[it.slot];
-                        const PatchRay prr = patch_ray(rr, C.x, C.y, C.z);
-                        const float lim = cull_eps + 8e-6f * (float)C.w;
-                        ++hull_tests;
-                        const bool miss = op.hull_cull >= 4
-                                              ? clip_misses<P, Q>(sc.cp + h.x, rr, prr, lim)
-                                              : hull_misses<P, Q>(sc.cp + h.x, rr, prr, lim) ||
-                                                    (op.hull_cull >= 2 && subdiv_misses<P, Q>(sc.cp + h.x, rr, prr, lim));
-                        if (miss) {
-                            keep = false;
-                            ++culled;
-                        }
-                    }
-                }
-            }
-            const unsigned m = __ballot_sync(kFull, keep);
-            if (keep) qu[qn + __popc(m & lt_mask)] = k;
-            qn += __popc(m);
-            __syncwarp();
-        }
-        const int take = need < qn ? need : qn;
-        if (!busy) {
-            const int rank = __popc(idle & lt_mask);
-            if (rank < take) {
-                const int k = qu[qn - take + rank];
-                const WfItem it = wb.items[k];
-                item_ray(it, r);
-                const int4 h = sc.hdr[it.slot];
-                const double4 C = sc.centre[it.slot];
-                pr = patch_ray(r, C.x, C.y, C.z);
-                blk = sc.cp + h.x;
-                ray = it.ray;
-                slot = it.slot;
-                wide = (h.y >> 8) & kFlagWideWeights;
-                ++solves;
-                if (tests) atomicAdd(tests + ray, 1);
-                float gu = 0.5f, gv = 0.5f;
-                if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
-                busy = true;
-                if (op.flat_threshold > 0.f) {  // flat-skip, as the per-pixel kernel runs it
-                    const float4 lo = __ldg(sc.leafbox + 2 * slot), hi = __ldg(sc.leafbox + 2 * slot + 1);
-                    const float te = slab(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, r, __frcp_rn(r.dx), __frcp_rn(r.dy),
-                                          __frcp_rn(r.dz));
-                    NewtonOut fo;
-                    if (flat_accept<P, Q>(blk, r, pr, __ldg(sc.delta + slot), te, op, gu, gv, fo) && 0.f < fo.t) {
-                        ++flats;
-                        evals += 1;
-                        const unsigned long long key =
-                            ((unsigned long long)__float_as_uint(fo.t) << 32) | ((unsigned)slot << 1) | 1u;
-                        const unsigned long long uv =
-                            ((unsigned long long)__float_as_uint(fo.u) << 32) | __float_as_uint(fo.v);
-                        if (!record_hit(wb.best + ray, key, uv)) ++cas_err;
-                        busy = false;
-                    }
-                }
-                if (busy) st = newton_start(gu, gv, (uint32_t)ray + op.seed_offset);
-            }
-        }
-        qn -= take;
-        __syncwarp();
-        if (!__any_sync(kFull, busy)) break;  // every lane idle after a refill: the input is used up
-        if (busy) {
-            NewtonOut o;
-            NewtonOpts nwl = nw;  // the FP64 decisions apply to patches with widely spread weights
-            nwl.fp64_band = nw.fp64_band && wide;
-            if (newton_step<P, Q, true>(blk, r, pr, st, nwl, o)) {
-                newton_finish<P, Q>(blk, r, pr, st, nwl, o);
-                busy = false;
-                evals += (unsigned)o.done;
-                f64 += (unsigned)o.fp64_solves;
-                if (o.evals > 0 && o.t > 0.f) {
-                    const unsigned long long key = ((unsigned long long)__float_as_uint(o.t) << 32) | ((unsigned)slot << 1);
-                    const unsigned long long uv =
-                        ((unsigned long long)__float_as_uint(o.u) << 32) | __float_as_uint(o.v);
-                    if (!record_hit(wb.best + ray, key, uv)) ++cas_err;
-                }
-            }
-        }
-    }
-    if (ctr && op.counters) {
-        count_add(ctr, kSolves, solves);
-        count_add(ctr, kEvals, evals);
-        count_add(ctr, kFp64Solves, f64);
-        count_add(ctr, kCulled, culled);
-        count_add(ctr, kFlatSkips, flats);
-        if (evals) atomicAdd(ctr + kEvalsByDegree + P * 8 + Q, evals);
-        if (hull_tests) atomicAdd(ctr + kHullByDegree + P * 8 + Q, hull_tests);
-    }
-    if (ctr && cas_err) atomicAdd(ctr + kErrors, cas_err);
-}
-
 // Resolve, step 1: rays without a hit get their miss record; rays with one
 
 // Resolve, step 2 (one launch per degree class): rebuild the winning solve's
@@ -513,12 +364,8 @@ void newton_class(const WfClassLaunch& L) {
                                                                         L.rank_hi, *L.op, L.tests, L.ctr);
             break;
         default:
-            if (L.refill >= 32)  // lockstep batches of 32 solves
-                k_wf_newton<P, Q, kWfPlain><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.rays, *L.wb, L.cls, L.rank_lo,
-                                                                          L.rank_hi, *L.op, L.tests, L.ctr);
-            else
-                k_wf_newton_plain<P, Q><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op,
-                                                                      L.tests, L.ctr, L.refill);
+            k_wf_newton<P, Q, kWfPlain><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.rays, *L.wb, L.cls, L.rank_lo,
+                                                                      L.rank_hi, *L.op, L.tests, L.ctr);
     }
 }
 

@@ -6,10 +6,20 @@ cond(J) > 1e4) and the FP64 final step.
 
 Two references:
   * the FP64 oracle (the same method in double, TEST INFRASTRUCTURE) judges
-    hit/miss.  On these nets Newton's basins are chaotic (degree 7, a 1e4
-    weight ratio, steep relief): FP32 and FP64 iterations from the same start
-    part ways on a fraction of a percent of rays, with or without the FP64
-    steps, so agreement is asserted at >= 99% and reported;
+    hit/miss.  Every disagreement is classified against the true closest hit
+    (oracle.true_closest_hits: a 4 x 4 lattice of FP64 Newton starts plus the
+    midpoint on every patch the ray's box test admits) and by the evaluation
+    at which the deciding solve converged.  What remains are solves that need
+    the whole 8-evaluation budget from the midpoint: there FP32 and FP64
+    iterations from the same start part ways (degree 7, a 1e4 weight ratio,
+    steep relief) and one converges at the last evaluation while the other
+    needs a ninth.  Measured on this workload: agreement 99.87 % with the FP64
+    decision band (FP32 alone 99.64 %; the FP32 restatement of the reference's
+    own algorithm agrees with the FP64 oracle on 98.73 %), and the engine
+    agrees with the true closest hit as often as the FP64 oracle does (within
+    0.1 %).  Asserted: agreement >= 99.85 %, grazing rays >= 99.8 %, and at
+    least 80 % of the disagreeing solves decided at one of the last two
+    evaluations of the budget;
   * the exact root next to each GPU hit (FP64 Newton from the GPU's (u, v),
     converged to 1e-13 in double, numpy) gives the t and (u, v) error of the
     returned hits.  With the FP64 final step: relative t error <= 5e-6 at the
@@ -113,7 +123,28 @@ def test_precision_stress(nrt_gpu, oracle_mod):
           "p99.99", np.quantile(rel32, 0.9999), "uv p99.99", np.quantile(duv32, 0.9999),
           "| FP64 solve fraction", round(fp64_frac, 5), "| exact root found for", round(conv, 5))
     assert st["hit_rate"] > 0.2 and stg["hit_rate"] > 0.5, (st, stg)
-    assert st["agree"] >= 0.99 and stg["agree"] >= 0.99, (st, stg)
+    assert st["agree"] >= 0.9985 and stg["agree"] >= 0.998, (st, stg)
+    # the disagreements, classified
+    dis = np.nonzero((out["patch"] >= 0) != (ref.patch >= 0))[0]
+    r_dis = oracle_mod.Rays(*[np.ascontiguousarray(a[dis]) for a in rays_np])
+    tr = oracle_mod.true_closest_hits(P, r_dis, grid=4)
+    he, ho, ht = out["patch"][dis] >= 0, ref.patch[dis] >= 0, tr.patch >= 0
+    engine_iters = np.where(he, out["iters"][dis], 0)
+    oracle_iters = np.where(ho, ref.evals[dis], 0)
+    late = np.where(he, engine_iters, oracle_iters) >= 7
+    cls = {"engine hit = true closest": int((he & ht & (np.abs(out["t"][dis] - tr.t) <= 1e-4 * tr.t)).sum()),
+           "engine hit, farther root": int((he & ~(ht & (np.abs(out["t"][dis] - tr.t) <= 1e-4 * tr.t))).sum()),
+           "oracle hit = true closest": int((ho & ht & (np.abs(ref.t[dis] - tr.t) <= 1e-4 * tr.t)).sum()),
+           "oracle hit, farther root": int((ho & ~(ht & (np.abs(ref.t[dis] - tr.t) <= 1e-4 * tr.t))).sum())}
+    # every 13th ray: camera and grazing rays in their proportions (grazing rays are every 4th)
+    whole = oracle_mod.true_closest_hits(P, oracle_mod.Rays(*[np.ascontiguousarray(a[::13]) for a in rays_np]), grid=4)
+    t_has = whole.patch >= 0
+    agree_true = {"engine": float(((out["patch"][::13] >= 0) == t_has).mean()),
+                  "fp64 oracle": float(((ref.patch[::13] >= 0) == t_has).mean())}
+    print("precision stress disagreements:", dis.size, cls, "decided at evaluation 7-8:", int(late.sum()),
+          "| hit/miss against the true closest hit (every 13th ray):", agree_true)
+    assert late.mean() >= 0.8, (late.mean(), cls)
+    assert abs(agree_true["engine"] - agree_true["fp64 oracle"]) <= 1e-3, agree_true
     assert conv > 0.999
     assert np.quantile(rel, 0.999) <= 5e-6 and np.quantile(rel, 0.9999) <= 2e-5, np.quantile(rel, [0.999, 0.9999])
     assert (rel > 1e-4).mean() <= 1e-4 and rel.max() <= 2e-3, ((rel > 1e-4).sum(), rel.max())
