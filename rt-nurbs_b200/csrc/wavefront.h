@@ -30,8 +30,7 @@ __host__ __device__ constexpr int round_quota(int r, int q0 = 1, int qmax = 8) {
 
 // Scratch of one wavefront launch over n rays (device pointers).
 struct WfBuffers {
-    int32_t* stack_ref;            // kStack * n, entry k of ray i at [k * n + i]
-    float* stack_t;                // kStack * n
+    int2* stack;                   // kStack * n (node, entry distance bits), entry k of ray i at [k * n + i]
     int32_t* stack_sp;             // n
     ulonglong2* best;              // n: the nearest hit so far, {key, (u bits << 32) | v bits}; the key
                                    // (t bits << 32) | slot << 1 | flat orders hits by t, then slot

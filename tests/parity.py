@@ -56,7 +56,9 @@ def root_stats(oracle_mod, P, rays_np, got, ref, cosang=None):
     reported (u, v) on the reported patch; the oracle itself stops at the
     method's eps, so its t is only good to about eps / sin(angle)).  Returns:
     genuine (fraction of engine hits that refine to a root), t_err / uv_err
-    (engine hit against its exact root; max and quantiles; with cosang, the
+    (engine hit against its exact root, t relative to t or to 1e4 FP32 ulps of
+    the ray origin's largest coordinate, whichever is larger; max and
+    quantiles; with cosang, the
     |cos| of each hit's crossing angle, t_err_max is taken over the hits with
     |cos| >= 1e-2 and t_err_tangent counts the others above 1e-4), same_root
     (fraction of rays both hit where the two exact roots coincide) and the
@@ -68,7 +70,13 @@ def root_stats(oracle_mod, P, rays_np, got, ref, cosang=None):
     ok = he & (pe.patch >= 0)
     st = {"genuine": float(ok.sum() / max(he.sum(), 1))}
     if ok.any():
-        rel = np.abs(got["t"][ok].astype(np.float64) - pe.t[ok]) / np.abs(pe.t[ok])
+        # An absolute error below one FP32 ulp of the origin's largest
+        # coordinate is not counted against t: the hit point o + t d cannot be
+        # stored more finely than that (it matters only for rays that end very
+        # near their origin, such as bounce rays reaching the next patch of a
+        # crease at t ~ 1e-6).
+        o_ulp = np.spacing(np.max(np.abs(np.stack(rays_np[:3], 1)), axis=1).astype(np.float32)).astype(np.float64)
+        rel = np.abs(got["t"][ok].astype(np.float64) - pe.t[ok]) / np.maximum(np.abs(pe.t[ok]), 1e4 * o_ulp[ok])
         duv = np.maximum(np.abs(got["u"][ok] - pe.u[ok]), np.abs(got["v"][ok] - pe.v[ok]))
         wc = np.ones(rel.size, bool) if cosang is None else cosang[ok] >= 1e-2
         st.update({"t_err_max": float(rel[wc].max()) if wc.any() else 0.0,

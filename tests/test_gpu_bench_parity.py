@@ -14,7 +14,10 @@ the bench times them (through the C ABI).
 Tolerance (the stated target): hit/miss agreement >= 99.99 % with the FP64
 oracle; the same root (same patch, coinciding exact roots) on >= 99.9 % of
 the rays both hit; every reported hit a genuine root (>= 99.99 % refine to
-one) with relative t error <= 1e-4 against that exact root, and (u, v) within
+one) with relative t error <= 1e-4 against that exact root (or an absolute
+error within one FP32 ulp of the ray origin's largest coordinate, the finest
+the hit point o + t d can be stored: bounce rays that reach the next patch of
+a crease end at t ~ 1e-6 of their origin), and (u, v) within
 1e-4 at the 99.9th percentile.  t is measured against the exact root, not
 against the oracle's own t: the oracle stops at |r1|+|r2| < 1e-6, which on a
 short or grazing ray is more than 1e-4 of t.  The t bound holds for every hit
