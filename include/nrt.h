@@ -191,10 +191,12 @@ typedef struct {
     int hull_cull;        /* skip (ray, patch) tests that provably cannot converge (results
                              unchanged): 1 control points all on one side of a ray plane by
                              more than eps; 2 also each half net split at u or v = 1/2;
-                             wavefront only: 3 as 2, after an oriented-box test of each
-                             patch during traversal; 4 the box test, then the exact 2D
-                             hull of the plane residuals and of both halves of the net
-                             split at u = 1/2, or at v = 1/2 */
+                             wavefront only: 3 an oriented-box test of each patch during
+                             traversal, and no per-pair test after it (the fastest: the
+                             per-pair tests cost more than the solves they remove once the
+                             box test has run; the per-pixel schedule runs level 1 for it);
+                             4 the box test, then the exact 2D hull of the plane residuals
+                             and of both halves of the net split at u = 1/2, or at v = 1/2 */
     int schedule;         /* NRT_SCHED_PIXEL or NRT_SCHED_WAVEFRONT */
     int seed_offset;      /* added to the ray index to seed the singular-Jacobian pull */
     float flat_threshold; /* flat-skip in pixels (src/gpu/intersect.cu:104-123); 0 = off.  Both

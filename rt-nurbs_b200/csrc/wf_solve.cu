@@ -137,7 +137,10 @@ __global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuf
             bool keep = false;
             if (k < end) {
                 keep = true;
-                if (op.hull_cull) {
+                // level 3 is the traversal's oriented-box test alone: after it the per-pair
+                // hull tests cost more than the solves they remove (16.4 against 18.3 ms per
+                // step on the 64-surface workload, with the same hits)
+                if (op.hull_cull && op.hull_cull != 3) {
                     const WfItem it = wb.items[k];
                     const int4 h = sc.hdr[it.slot];
                     if ((h.y >> 8) & kFlagPositiveWeights) {
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuf
                         const bool miss = op.hull_cull >= 4
                                               ? clip_misses<P, Q>(sc.cp + h.x, r, pr, lim)
                                               : hull_misses<P, Q>(sc.cp + h.x, r, pr, lim) ||
-                                                    (op.hull_cull >= 2 && subdiv_misses<P, Q>(sc.cp + h.x, r, pr, lim));
+                                                    (op.hull_cull == 2 && subdiv_misses<P, Q>(sc.cp + h.x, r, pr, lim));
                         if (miss) {
                             keep = false;
                             ++culled;
