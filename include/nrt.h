@@ -122,7 +122,7 @@ typedef struct {
     int max_leaf;       /* patches per BVH leaf (1..8, default 1) */
     int device;         /* CUDA device ordinal */
     int64_t wavefront_chunk; /* rays per wavefront pass (0 = 2^23); bounds its scratch,
-                                about 540 bytes per ray, allocated on first use */
+                                about 1.1 KB per ray, allocated on first use */
 } nrt_build_opts;
 
 int nrt_scene_create(const nrt_nurbs_surface* surfaces, int n_surfaces, const nrt_build_opts* opts,
@@ -247,13 +247,13 @@ int nrt_intersect_noalloc(nrt_scene* scene, const nrt_rays* rays, int64_t n, con
  * src/gpu/intersect.cu:205-217).  In nrt_scene_set_tuning a field <= 0 keeps
  * its current value. */
 typedef struct {
-    int64_t step_blocks;     /* traversal kernel in the graph: persistent blocks of 128 threads that
-                                take 128 active rays at a time */
+    int64_t step_blocks;     /* traversal kernel in the graph: persistent blocks of 128 threads whose
+                                warps take 32 active rays at a time */
     int64_t scatter_blocks;  /* work-item scatter in the graph: persistent blocks of 256 threads */
     int32_t class_blocks;    /* blocks of 256 threads per degree-class Newton launch */
     int32_t graph;           /* 1: rounds run inside one CUDA graph with a device-side loop (no host
                                 synchronisation); 2: host-driven rounds (one synchronisation each) */
-    int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 540 bytes per ray) */
+    int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 1.1 KB per ray) */
     int32_t quota0;          /* candidates a ray emits in the first round, doubling per round ... */
     int32_t quota_max;       /* ... up to this many (<= 8); the default 4, then 8 */
 } nrt_wavefront_tuning;

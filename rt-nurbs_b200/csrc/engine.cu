@@ -90,6 +90,8 @@ struct nrt_scene {
     std::vector<WfGraph> wf_graphs;
     long long wf_graph_passes = 0;  // passes of the graph the last call ran
     bool last_graph = false;     // the last nrt_intersect ran the graph (rounds counted on the device)
+    int last_guess_round = 0;    // ... and its guess kernels (learned mode): per round, and per pass
+    int last_guess_pass = 0;
     dev::WfTuning tuning{};
     bool use_graph = true;       // false: host-driven rounds
     bool timing_on = false;      // events around the per-class Newton launches (host-driven rounds)
@@ -668,6 +670,8 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
             scene->wf_graph_passes = gs[at].passes;
         }
         scene->last_graph = true;
+        scene->last_guess_round = o.init_mode == NRT_INIT_LEARNED ? 1 : 0;
+        scene->last_guess_pass = (o.init_mode == NRT_INIT_LEARNED && hits->iters) ? 1 : 0;
     }
     if (prev != scene->device) cudaSetDevice(prev);
     if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
@@ -833,7 +837,8 @@ int nrt_get_counters(nrt_scene* scene, nrt_counters* out, void* stream) {
     out->learned_fallback_converged = h[dev::kFallbackConverged];
     out->flat_skips = h[dev::kFlatSkips];
     if (scene->last_graph) {  // rounds counted on the device; kernels per pass and per round are fixed
-        const uint64_t per_pass = 4 + (uint64_t)scene->plan.n_classes, per_round = 4 + (uint64_t)scene->plan.n_classes;
+        const uint64_t nc = (uint64_t)scene->plan.n_classes;
+        const uint64_t per_pass = 4 + nc * (1 + scene->last_guess_pass), per_round = 4 + nc * (1 + scene->last_guess_round);
         out->rounds = h[dev::kRoundsDone];
         out->kernel_launches = (uint64_t)scene->wf_graph_passes * per_pass + out->rounds * per_round;
     } else {

@@ -330,7 +330,7 @@ size_t wavefront_scratch_bytes(long long n, int n_slots) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t N = (size_t)n, S = (size_t)n_slots + 1;
     return al(N * kStack * 8) + al(N * 4) + al(N * 16) + 2 * al(N * 4) + al(32) + al(N * kEmitMax * 4) +
-           al(N * 4) + al(N * kEmitMax * sizeof(WfItem)) + 3 * al(S * 4) + al(64 * 4);
+           al(N * 4) + al(N * kEmitMax * sizeof(WfItem)) + al(N * kEmitMax * 8) + 3 * al(S * 4) + al(64 * 4);
 }
 
 WfBuffers wavefront_carve(void* base, long long n, int n_slots) {
@@ -347,6 +347,7 @@ WfBuffers wavefront_carve(void* base, long long n, int n_slots) {
     b.emit_slot = reinterpret_cast<int32_t*>(p); p += al(N * kEmitMax * 4);
     b.emit_cnt = reinterpret_cast<int32_t*>(p); p += al(N * 4);
     b.items = reinterpret_cast<WfItem*>(p); p += al(N * kEmitMax * sizeof(WfItem));
+    b.guess = reinterpret_cast<float2*>(p); p += al(N * kEmitMax * 8);
     b.hist = reinterpret_cast<int32_t*>(p); p += al(S * 4);
     b.cursor = reinterpret_cast<int32_t*>(p); p += al(S * 4);
     b.offsets = reinterpret_cast<int32_t*>(p); p += al(S * 4);
@@ -403,7 +404,7 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         k_wf_scan<<<1, 1024, 0, stream>>>(plan.n_slots, wb);
         k_wf_scatter<<<(unsigned)((n_active + 255) / 256), 256, 0, stream>>>(rays, round, n_active, wb, cur,
                                                                              plan.rank_of);
-        *launches += 3 + plan.n_classes;
+        *launches += 3 + plan.n_classes * (L.mode == kWfLearned ? 2 : 1);  // learned: the guess kernels too
         *rounds += 1;
         const bool timed = ev && newton_ms;
         if (timed) cudaEventRecord(ev[0], stream);
@@ -441,7 +442,7 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         L.grid = plan.class_grid[c];
         wf_resolve_class(plan.class_pq[c] & 15, plan.class_pq[c] >> 4, L);
     }
-    *launches += 3 + plan.n_classes;
+    *launches += 3 + plan.n_classes * ((L.mode == kWfLearned && out.iters) ? 2 : 1);
     return cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ struct WfBuffers {
     int32_t* emit_slot;            // n * kEmitMax: candidates emitted this round, by active position
     int32_t* emit_cnt;             // n
     WfItem* items;                 // n * kEmitMax: work items of a round, in rank order
+    float2* guess;                 // n * kEmitMax: the network's raw (u, v) for each work item (learned guess)
     int32_t* hist;                 // n_slots + 1
     int32_t* cursor;               // n_slots + 1
     int32_t* offsets;              // n_slots + 1

@@ -95,6 +95,46 @@ __device__ __forceinline__ void item_features(const Scene& sc, bool valid, int s
     if (valid) features(sc.frames[slot], h.y & 15, (h.y >> 4) & 15, r, pr, C.x, C.y, C.z, x);
 }
 
+// The network's raw (u, v) guess for every work item in [offsets[rank_lo],
+// offsets[rank_hi]) into wb.guess (learned mode).  Inference is
+// warp-synchronous (mma.sync on the warp's 32 items); it runs here, in a
+// kernel whose warps never diverge, and not inside the Newton kernels, whose
+// lanes leave their solves at different times: there the tensor-core
+// instructions were not always reached by the whole warp at once, and the
+// learned kernels stalled.
+template <int P, int Q>
+__global__ void __launch_bounds__(256) k_wf_guess(Scene sc, WfBuffers wb, int rank_lo, int rank_hi, Opts op) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    MlpSmem* ms = reinterpret_cast<MlpSmem*>(dyn_smem);
+    mlp_load(*ms, op.mlp);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
+    for (long long base = begin + ((long long)blockIdx.x * 8 + warp) * 32; base < end;
+         base += (long long)gridDim.x * 256) {
+        const long long k = base + lane;
+        const bool valid = k < end;
+        RayFrame r;
+        int4 h = make_int4(0, 0, 0, 0);
+        double4 C = make_double4(0.0, 0.0, 0.0, 0.0);
+        PatchRay pr{};
+        int slot = 0;
+        if (valid) {
+            const WfItem it = wb.items[k];
+            item_ray(it, r);
+            slot = it.slot;
+            h = sc.hdr[slot];
+            C = sc.centre[slot];
+            pr = patch_ray(r, C.x, C.y, C.z);
+        }
+        float x[kMlpIn];
+        item_features(sc, valid, slot, h, C, r, pr, x);
+        float lu, lv;
+        mlp_infer_warp(*ms, warp, lane, x, lu, lv);
+        if (valid) wb.guess[k] = make_float2(lu, lv);
+    }
+}
+
 // Newton over the items of one degree class.  Each warp takes 32 items at a
 // time (chunks in a fixed stride), runs the hull tests on them (one lane per item;
 // the items of a warp mostly share a patch, so control point loads broadcast),
@@ -104,14 +144,8 @@ template <int P, int Q, int MODE>
 __global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
                                                    int rank_hi, Opts op, int32_t* tests, unsigned long long* ctr) {
     constexpr unsigned kFull = 0xffffffffu;
-    constexpr bool kUseNet = MODE == kWfLearned, kFeatures = MODE != kWfPlain;
+    constexpr bool kUseNet = MODE == kWfLearned;
     __shared__ int queue[8][64];
-    extern __shared__ __align__(16) unsigned char dyn_smem[];  // the network, in the learned mode
-    MlpSmem* ms = reinterpret_cast<MlpSmem*>(dyn_smem);
-    if constexpr (kUseNet) {
-        mlp_load(*ms, op.mlp);
-        __syncthreads();
-    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* qu = queue[warp];
     const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
@@ -185,8 +219,14 @@ __global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuf
         }
         float x[kMlpIn];
         float lu = 0.5f, lv = 0.5f;
-        if constexpr (kFeatures) item_features(sc, k >= 0, k >= 0 ? it.slot : 0, h, C, r, pr, x);
-        if constexpr (kUseNet) mlp_infer_warp(*ms, warp, lane, x, lu, lv);  // warp-synchronous
+        if constexpr (MODE == kWfCollect) item_features(sc, k >= 0, k >= 0 ? it.slot : 0, h, C, r, pr, x);
+        if constexpr (kUseNet) {
+            if (k >= 0) {  // the network's guess, from k_wf_guess
+                const float2 g = wb.guess[k];
+                lu = g.x;
+                lv = g.y;
+            }
+        }
         if (k >= 0) {
             int fell = 0;
             const NewtonOut o = solve_item<P, Q, kUseNet>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv,
@@ -245,12 +285,6 @@ __global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuf
 template <int P, int Q, bool LEARNED>
 __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int rank_lo, int rank_hi, Opts op,
                                                     Hits out, unsigned long long* ctr) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    MlpSmem* ms = reinterpret_cast<MlpSmem*>(dyn_smem);
-    if constexpr (LEARNED) {
-        mlp_load(*ms, op.mlp);
-        __syncthreads();
-    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int begin = wb.offsets[rank_lo], end = wb.offsets[rank_hi];
     unsigned long long f64f = 0, hits = 0, err = 0;
@@ -270,16 +304,16 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
             C = sc.centre[it.slot];
             pr = patch_ray(r, C.x, C.y, C.z);
         }
-        float lu = 0.5f, lv = 0.5f;
-        if constexpr (LEARNED) {
-            float x[kMlpIn];
-            item_features(sc, valid, valid ? it.slot : 0, h, C, r, pr, x);
-            mlp_infer_warp(*ms, warp, lane, x, lu, lv);
-        }
-        if (valid) {  // idle lanes wait at the __syncwarp below, so the next mma runs converged
+        if (valid) {
         const long long i = it.ray;
         NewtonOut o;
         if (out.iters) {  // the evaluation count is wanted: solve again
+            float lu = 0.5f, lv = 0.5f;
+            if constexpr (LEARNED) {  // the network's guess, from k_wf_guess over these items
+                const float2 g = wb.guess[k];
+                lu = g.x;
+                lv = g.y;
+            }
             int fell = 0;
             o = solve_item<P, Q, LEARNED>(sc, it.slot, r, pr, sc.cp + h.x, lu, lv, (uint32_t)it.ray + op.seed_offset,
                                           op, op.nw, fell);
@@ -340,8 +374,6 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
 }
 
 // Dynamic shared memory for the network: the attribute is set once per kernel
-
-// Dynamic shared memory for the network: the attribute is set once per kernel
 // (per process; every kernel of this file runs on devices of one architecture).
 template <class K>
 void allow_mlp_smem(K kernel, bool& done) {
@@ -357,9 +389,10 @@ void newton_class(const WfClassLaunch& L) {
     switch (L.mode) {
         case kWfLearned: {
             static bool done = false;
-            allow_mlp_smem(k_wf_newton<P, Q, kWfLearned>, done);
-            k_wf_newton<P, Q, kWfLearned><<<L.grid, 256, sizeof(MlpSmem), L.stream>>>(
-                *L.sc, *L.rays, *L.wb, L.cls, L.rank_lo, L.rank_hi, *L.op, L.tests, L.ctr);
+            allow_mlp_smem(k_wf_guess<P, Q>, done);
+            k_wf_guess<P, Q><<<L.grid, 256, sizeof(MlpSmem), L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op);
+            k_wf_newton<P, Q, kWfLearned><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.rays, *L.wb, L.cls, L.rank_lo,
+                                                                        L.rank_hi, *L.op, L.tests, L.ctr);
             break;
         }
         case kWfCollect:
@@ -376,10 +409,13 @@ template <int Q>
 void resolve_class(const WfClassLaunch& L) {
     constexpr int P = NRT_WF_P;
     if (L.mode == kWfLearned) {
-        static bool done = false;
-        allow_mlp_smem(k_wf_resolve<P, Q, true>, done);
-        k_wf_resolve<P, Q, true><<<L.grid, 256, sizeof(MlpSmem), L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi,
-                                                                             *L.op, *L.out, L.ctr);
+        if (L.out->iters) {  // the winners are solved again: their guesses first
+            static bool done = false;
+            allow_mlp_smem(k_wf_guess<P, Q>, done);
+            k_wf_guess<P, Q><<<L.grid, 256, sizeof(MlpSmem), L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op);
+        }
+        k_wf_resolve<P, Q, true><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op, *L.out,
+                                                               L.ctr);
     } else {
         k_wf_resolve<P, Q, false><<<L.grid, 256, 0, L.stream>>>(*L.sc, *L.wb, L.rank_lo, L.rank_hi, *L.op, *L.out,
                                                                 L.ctr);
