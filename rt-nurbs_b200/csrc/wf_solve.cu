@@ -44,30 +44,49 @@ __device__ __forceinline__ NewtonOut solve_item(const Scene& sc, int slot, const
     fell_back = 0;
     NewtonOpts nw = nw_in;  // the FP64 decisions apply to patches with widely spread weights
     nw.fp64_band = nw_in.fp64_band && ((__ldg(&sc.hdr[slot].y) >> 8) & kFlagWideWeights);
-    const bool inside = lu >= -0.25f && lu <= 1.25f && lv >= -0.25f && lv <= 1.25f;
-    if (LEARNED && inside) {
-        NewtonOpts nl = nw;
-        if (op.learned_iters > 0 && op.learned_iters < nw.max_iter) nl.max_iter = op.learned_iters;
-        const NewtonOut o = newton<P, Q>(blk, r, pr, fminf(fmaxf(lu, 0.f), 1.f), fminf(fmaxf(lv, 0.f), 1.f), seed, nl);
-        if (o.evals > 0) return o;
-        fell_back = 1;
-        NewtonOut f = newton<P, Q>(blk, r, pr, 0.5f, 0.5f, seed, nw);
-        f.evals = f.evals > 0 ? f.evals - o.evals : f.evals + o.evals;
-        f.fp64_solves += o.fp64_solves;
-        f.done += o.done;
-        return f;
-    }
-    if (LEARNED) fell_back = 2;  // gated off: plain Newton only
-    float gu = 0.5f, gv = 0.5f;
-    if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
-    if (!LEARNED && op.flat_threshold > 0.f) {
-        // the ray's entry into the slot's leaf box, computed as the traversal does
-        const float4 lo = __ldg(sc.leafbox + 2 * slot), hi = __ldg(sc.leafbox + 2 * slot + 1);
-        const float te = slab(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, r, __frcp_rn(r.dx), __frcp_rn(r.dy), __frcp_rn(r.dz));
+    if constexpr (LEARNED) {
+        // the attempts, through one call site (the solve is compiled once): from the network's
+        // guess for learned_iters evaluations, then from the midpoint with the full budget
+        const bool inside = lu >= -0.25f && lu <= 1.25f && lv >= -0.25f && lv <= 1.25f;
+        fell_back = inside ? 0 : 2;  // 2: gated off, plain Newton only
+        int first_evals = 0, first_f64 = 0, first_done = 0;
         NewtonOut o;
-        if (flat_accept<P, Q>(blk, r, pr, __ldg(sc.delta + slot), te, op, gu, gv, o) && 0.f < o.t) return o;
+        for (int attempt = inside ? 0 : 1; attempt < 2; ++attempt) {
+            NewtonOpts na = nw;
+            float u0 = 0.5f, v0 = 0.5f;
+            if (attempt == 0) {
+                if (op.learned_iters > 0 && op.learned_iters < nw.max_iter) na.max_iter = op.learned_iters;
+                u0 = fminf(fmaxf(lu, 0.f), 1.f);
+                v0 = fminf(fmaxf(lv, 0.f), 1.f);
+            }
+            o = newton<P, Q>(blk, r, pr, u0, v0, seed, na);
+            if (attempt == 0) {
+                if (o.evals > 0) return o;
+                fell_back = 1;
+                first_evals = o.evals;
+                first_f64 = o.fp64_solves;
+                first_done = o.done;
+            }
+        }
+        if (fell_back == 1) {
+            o.evals = o.evals > 0 ? o.evals - first_evals : o.evals + first_evals;
+            o.fp64_solves += first_f64;
+            o.done += first_done;
+        }
+        return o;
+    } else {
+        float gu = 0.5f, gv = 0.5f;
+        if (op.init_mode == 1) bilinear_guess(sc.corners + 4 * slot, r, gu, gv);
+        if (op.flat_threshold > 0.f) {
+            // the ray's entry into the slot's leaf box, computed as the traversal does
+            const float4 lo = __ldg(sc.leafbox + 2 * slot), hi = __ldg(sc.leafbox + 2 * slot + 1);
+            const float te =
+                slab(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, r, __frcp_rn(r.dx), __frcp_rn(r.dy), __frcp_rn(r.dz));
+            NewtonOut o;
+            if (flat_accept<P, Q>(blk, r, pr, __ldg(sc.delta + slot), te, op, gu, gv, o) && 0.f < o.t) return o;
+        }
+        return newton<P, Q>(blk, r, pr, gu, gv, seed, nw);
     }
-    return newton<P, Q>(blk, r, pr, gu, gv, seed, nw);
 }
 
 // Lower the ray's nearest-hit record to {key, uv} if key is smaller: a 128-bit
@@ -141,7 +160,7 @@ __global__ void __launch_bounds__(256) k_wf_guess(Scene sc, WfBuffers wb, int ra
 // and queues the survivors in shared memory; Newton then runs on full warps of
 // survivors, so culled items do not leave lanes idle.
 template <int P, int Q, int MODE>
-__global__ void __launch_bounds__(256, 2) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
+__global__ void __launch_bounds__(256, MODE == kWfPlain ? 2 : 1) k_wf_newton(Scene sc, Rays rays, WfBuffers wb, int cls, int rank_lo,
                                                    int rank_hi, Opts op, int32_t* tests, unsigned long long* ctr) {
     constexpr unsigned kFull = 0xffffffffu;
     constexpr bool kUseNet = MODE == kWfLearned;
