@@ -69,7 +69,7 @@ __device__ __forceinline__ bool flat_accept(const float* __restrict__ blk, const
                                             float delta, float te, const Opts& op, float gu, float gv, NewtonOut& o) {
     if (!(op.flat_threshold > 0.f && delta * op.cam_k / te < op.flat_threshold)) return false;
     float H[4], Hu[4], Hv[4];
-    eval_patch<P, Q, float>(blk, gu, gv, H, Hu, Hv);
+    eval_patch<P, Q>(blk, gu, gv, H, Hu, Hv);
     const float iw = __frcp_rn(H[3]);
     const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
     const float r1 = fmaf(r.n1x, sx, fmaf(r.n1y, sy, fmaf(r.n1z, sz, pr.e1)));

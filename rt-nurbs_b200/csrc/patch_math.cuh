@@ -2,8 +2,11 @@
 //
 // Patches live on the device in patch-local coordinates: every patch has a
 // centre C (double) and its control points are stored as
-// (w*(x-Cx), w*(y-Cy), w*(z-Cz), w) in FP32, one SoA block per patch
-// (X[np] Y[np] Z[np] W[np], np = (p+1)(q+1) rounded up to 4, 16-byte aligned).
+// (w*(x-Cx), w*(y-Cy), w*(z-Cz), w) in FP32, one block per patch of two
+// halves, XY = X0 Y0 X1 Y1 ... and ZW = Z0 W0 Z1 W1 ... (np = (p+1)(q+1)
+// rounded up to 4 points per coordinate, 16-byte aligned): a 16-byte load
+// brings two points' (x, y) or (z, w) pairs, the operand pairs of the paired
+// FP32 instructions that evaluate two coordinates at once.
 // The ray's two planes n_k.x + d_k = 0 (MathUtils::getRayPlanes,
 // src/math/math_utils.h:33-54) become n_k.S_loc + e_k with e_k = -n_k.(O - C)
 // computed in FP64 once per (ray, patch); |e_k| is the distance from the ray to
@@ -21,6 +24,10 @@ namespace dev {
 constexpr int kMaxDeg = 7;
 
 __host__ __device__ constexpr int padded_points(int p, int q) { return (((p + 1) * (q + 1)) + 3) & ~3; }
+
+// Offsets (floats) of point k's coordinates in a block of np padded points:
+// coordinate a = 0..3 (x, y, z, w) of point k is at block_at(np, k, a).
+__host__ __device__ constexpr int block_at(int np, int k, int a) { return (a >> 1) * 2 * np + 2 * k + (a & 1); }
 
 __device__ __forceinline__ float fmx(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fmx(double a, double b, double c) { return ::fma(a, b, c); }
@@ -137,65 +144,84 @@ __device__ __forceinline__ void bernstein(T t, T (&B)[N + 1], T (&dB)[N + 1]) {
     }
 }
 
-// Tensor-product rational Bezier evaluation of one homogeneous coordinate as
-// a Bernstein sum: each row i is summed along v with the basis values and
-// their derivatives (the row point and its v-derivative), then the rows are
-// summed along u.  H, dH/du, dH/dv cost 2(p+1)(q+1) + 3(p+1) multiply-adds,
+// Tensor-product rational Bezier evaluation as a Bernstein sum: each row i
+// of the net is summed along v with the basis values and their derivatives
+// (the row point and its v-derivative), then the rows are summed along u.  H,
+// dH/du, dH/dv of one coordinate cost 2(p+1)(q+1) + 3(p+1) multiply-adds,
 // with the basis values computed once per (u, v) for all four coordinates;
 // the reference's BezierPatchEval (src/math/bezier_patch.h:172-191) runs two
 // full de Casteljau passes instead.
-template <int P, int Q, class T>
-__device__ __forceinline__ void eval_coord(const T (&c)[(P + 1) * (Q + 1)], const T (&Bu)[P + 1],
-                                           const T (&dBu)[P + 1], const T (&Bv)[Q + 1], const T (&dBv)[Q + 1], T& h,
-                                           T& hu, T& hv) {
+//
+// The four homogeneous coordinates are evaluated as two pairs, (x, y) and
+// (z, w), with the paired FP32 instructions of sm_100 (__fmul2_rn,
+// __ffma2_rn: one instruction, two round-to-nearest operations, each lane's
+// result that of the scalar __fmul_rn / __fmaf_rn): every multiply-add of the
+// sum serves two coordinates, and the block stores each point's pairs as
+// adjacent floats, so the operand pairs come straight from 16-byte loads.
+// Lane by lane the operations and their order are the scalar sum's.
+template <int P, int Q>
+__device__ __forceinline__ void eval_pair(const float2 (&c)[(P + 1) * (Q + 1)], const float (&Bu)[P + 1],
+                                          const float (&dBu)[P + 1], const float2 (&bv)[Q + 1],
+                                          const float2 (&dbv)[Q + 1], float2& h, float2& hu, float2& hv) {
 #pragma unroll
     for (int i = 0; i <= P; ++i) {
-        T r = Bv[0] * c[i * (Q + 1)], d = dBv[0] * c[i * (Q + 1)];
+        float2 r = __fmul2_rn(bv[0], c[i * (Q + 1)]), d = __fmul2_rn(dbv[0], c[i * (Q + 1)]);
 #pragma unroll
         for (int j = 1; j <= Q; ++j) {
-            r = fmx(Bv[j], c[i * (Q + 1) + j], r);
-            d = fmx(dBv[j], c[i * (Q + 1) + j], d);
+            r = __ffma2_rn(bv[j], c[i * (Q + 1) + j], r);
+            d = __ffma2_rn(dbv[j], c[i * (Q + 1) + j], d);
         }
+        const float2 bu = make_float2(Bu[i], Bu[i]), dbu = make_float2(dBu[i], dBu[i]);
         if (i == 0) {
-            h = Bu[0] * r;
-            hu = dBu[0] * r;
-            hv = Bu[0] * d;
+            h = __fmul2_rn(bu, r);
+            hu = __fmul2_rn(dbu, r);
+            hv = __fmul2_rn(bu, d);
         } else {
-            h = fmx(Bu[i], r, h);
-            hu = fmx(dBu[i], r, hu);
-            hv = fmx(Bu[i], d, hv);
+            h = __ffma2_rn(bu, r, h);
+            hu = __ffma2_rn(dbu, r, hu);
+            hv = __ffma2_rn(bu, d, hv);
         }
     }
 }
 
-// Load one coordinate array of a patch block with 16-byte loads.
-template <int P, int Q, class T>
-__device__ __forceinline__ void load_coord(const float* __restrict__ src, T (&c)[(P + 1) * (Q + 1)]) {
+// Load one half of a patch block (the (x, y) or the (z, w) pairs of all
+// points) with 16-byte loads, two points per load.
+template <int P, int Q>
+__device__ __forceinline__ void load_pairs(const float* __restrict__ src, float2 (&c)[(P + 1) * (Q + 1)]) {
     constexpr int N = (P + 1) * (Q + 1);
     constexpr int NP = padded_points(P, Q);
     const float4* s4 = reinterpret_cast<const float4*>(src);
 #pragma unroll
-    for (int k = 0; k < NP / 4; ++k) {
+    for (int k = 0; k < NP / 2; ++k) {
         const float4 f = __ldg(s4 + k);
-        if (4 * k + 0 < N) c[4 * k + 0] = (T)f.x;
-        if (4 * k + 1 < N) c[4 * k + 1] = (T)f.y;
-        if (4 * k + 2 < N) c[4 * k + 2] = (T)f.z;
-        if (4 * k + 3 < N) c[4 * k + 3] = (T)f.w;
+        if (2 * k + 0 < N) c[2 * k + 0] = make_float2(f.x, f.y);
+        if (2 * k + 1 < N) c[2 * k + 1] = make_float2(f.z, f.w);
     }
 }
 
-template <int P, int Q, class T>
-__device__ __forceinline__ void eval_patch(const float* __restrict__ blk, T u, T v, T (&H)[4], T (&Hu)[4],
-                                           T (&Hv)[4]) {
+// H, dH/du, dH/dv of the four homogeneous coordinates at (u, v), FP32.
+template <int P, int Q>
+__device__ __forceinline__ void eval_patch(const float* __restrict__ blk, float u, float v, float (&H)[4],
+                                           float (&Hu)[4], float (&Hv)[4]) {
     constexpr int NP = padded_points(P, Q);
-    T Bu[P + 1], dBu[P + 1], Bv[Q + 1], dBv[Q + 1];
-    bernstein<P, T>(u, Bu, dBu);
-    bernstein<Q, T>(v, Bv, dBv);
+    float Bu[P + 1], dBu[P + 1], Bv[Q + 1], dBv[Q + 1];
+    bernstein<P, float>(u, Bu, dBu);
+    bernstein<Q, float>(v, Bv, dBv);
+    float2 bv[Q + 1], dbv[Q + 1];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        T c[(P + 1) * (Q + 1)];
-        load_coord<P, Q, T>(blk + a * NP, c);
-        eval_coord<P, Q, T>(c, Bu, dBu, Bv, dBv, H[a], Hu[a], Hv[a]);
+    for (int j = 0; j <= Q; ++j) {
+        bv[j] = make_float2(Bv[j], Bv[j]);
+        dbv[j] = make_float2(dBv[j], dBv[j]);
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {  // (x, y), then (z, w)
+        float2 c[(P + 1) * (Q + 1)];
+        load_pairs<P, Q>(blk + a * 2 * NP, c);
+        float2 h, hu, hv;
+        eval_pair<P, Q>(c, Bu, dBu, bv, dbv, h, hu, hv);
+        H[2 * a] = h.x; H[2 * a + 1] = h.y;
+        Hu[2 * a] = hu.x; Hu[2 * a + 1] = hu.y;
+        Hv[2 * a] = hv.x; Hv[2 * a + 1] = hv.y;
     }
 }
 
@@ -207,13 +233,13 @@ __device__ __forceinline__ void eval_patch_fp64(const float* __restrict__ blk, d
     constexpr int NP = padded_points(P, Q);
 #pragma unroll 1
     for (int a = 0; a < 4; ++a) {
-        const float* __restrict__ src = blk + a * NP;
+        const float* __restrict__ src = blk + block_at(NP, 0, a);  // coordinate a of point k at src[2 k]
         double pt[P + 1], dv[P + 1];
 #pragma unroll
         for (int i = 0; i <= P; ++i) {
             double r[Q + 1];
 #pragma unroll
-            for (int j = 0; j <= Q; ++j) r[j] = (double)__ldg(src + i * (Q + 1) + j);
+            for (int j = 0; j <= Q; ++j) r[j] = (double)__ldg(src + 2 * (i * (Q + 1) + j));
 #pragma unroll
             for (int k = 1; k < Q; ++k)
 #pragma unroll
@@ -249,19 +275,17 @@ __device__ __forceinline__ bool hull_misses(const float* __restrict__ blk, const
                                             float lim) {
     constexpr int N = (P + 1) * (Q + 1);
     constexpr int NP = padded_points(P, Q);
-    const float4* X = reinterpret_cast<const float4*>(blk);
-    const float4* Y = reinterpret_cast<const float4*>(blk + NP);
-    const float4* Z = reinterpret_cast<const float4*>(blk + 2 * NP);
-    const float4* W = reinterpret_cast<const float4*>(blk + 3 * NP);
+    const float4* XY = reinterpret_cast<const float4*>(blk);
+    const float4* ZW = reinterpret_cast<const float4*>(blk + 2 * NP);
     bool pos1 = true, neg1 = true, pos2 = true, neg2 = true;
 #pragma unroll
-    for (int k = 0; k < NP / 4; ++k) {
-        const float4 x = __ldg(X + k), y = __ldg(Y + k), z = __ldg(Z + k), w = __ldg(W + k);
-        const float xs[4] = {x.x, x.y, x.z, x.w}, ys[4] = {y.x, y.y, y.z, y.w};
-        const float zs[4] = {z.x, z.y, z.z, z.w}, ws[4] = {w.x, w.y, w.z, w.w};
+    for (int k = 0; k < NP / 2; ++k) {  // two points per pair of loads
+        const float4 xy = __ldg(XY + k), zw = __ldg(ZW + k);
+        const float xs[2] = {xy.x, xy.z}, ys[2] = {xy.y, xy.w};
+        const float zs[2] = {zw.x, zw.z}, ws[2] = {zw.y, zw.w};
 #pragma unroll
-        for (int l = 0; l < 4; ++l) {
-            if (4 * k + l >= N) break;
+        for (int l = 0; l < 2; ++l) {
+            if (2 * k + l >= N) break;
             const float a = fmaf(r.n1x, xs[l], fmaf(r.n1y, ys[l], fmaf(r.n1z, zs[l], pr.e1 * ws[l])));
             const float b = fmaf(r.n2x, xs[l], fmaf(r.n2y, ys[l], fmaf(r.n2z, zs[l], pr.e2 * ws[l])));
             const float m = lim * ws[l];
@@ -312,8 +336,10 @@ __device__ __forceinline__ bool subdiv_misses(const float* __restrict__ blk, con
                                               float lim) {
     constexpr int NP = padded_points(P, Q);
     auto coeff = [&](int k, float& a, float& b, float& w) {
-        const float x = __ldg(blk + k), y = __ldg(blk + NP + k), z = __ldg(blk + 2 * NP + k);
-        w = __ldg(blk + 3 * NP + k);
+        const float2 xy = __ldg(reinterpret_cast<const float2*>(blk) + k);
+        const float2 zw = __ldg(reinterpret_cast<const float2*>(blk + 2 * NP) + k);
+        const float x = xy.x, y = xy.y, z = zw.x;
+        w = zw.y;
         a = fmaf(r.n1x, x, fmaf(r.n1y, y, fmaf(r.n1z, z, pr.e1 * w)));
         b = fmaf(r.n2x, x, fmaf(r.n2y, y, fmaf(r.n2z, z, pr.e2 * w)));
     };
@@ -389,8 +415,10 @@ template <int P, int Q>
 __device__ __forceinline__ void residual_point(const float* __restrict__ blk, int k, const RayFrame& r,
                                                const PatchRay& pr, float& a, float& b, float& w) {
     constexpr int NP = padded_points(P, Q);
-    const float x = __ldg(blk + k), y = __ldg(blk + NP + k), z = __ldg(blk + 2 * NP + k);
-    w = __ldg(blk + 3 * NP + k);
+    const float2 xy = __ldg(reinterpret_cast<const float2*>(blk) + k);
+    const float2 zw = __ldg(reinterpret_cast<const float2*>(blk + 2 * NP) + k);
+    const float x = xy.x, y = xy.y, z = zw.x;
+    w = zw.y;
     a = fmaf(r.n1x, x, fmaf(r.n1y, y, fmaf(r.n1z, z, pr.e1 * w)));
     b = fmaf(r.n2x, x, fmaf(r.n2y, y, fmaf(r.n2z, z, pr.e2 * w)));
 }
@@ -790,7 +818,7 @@ __device__ __forceinline__ bool newton_step(const float* __restrict__ blk, const
     }
     const float u = s.u, v = s.v;
     float H[4], Hu[4], Hv[4];
-    eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
+    eval_patch<P, Q>(blk, u, v, H, Hu, Hv);
     ++s.done;
     const float iw = __frcp_rn(H[3]);
     const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;

@@ -216,8 +216,9 @@ NRT_HD inline dev::PatchFrame patch_frame(const float* P, int p, int q, double c
 }
 
 // Everything one slot stores, for patch `patch_id` of surface `surf` with
-// weighted-homogeneous points P (degree p, q) and box b, whose SoA block
-// starts `off` floats into the scene's block array; blk points there.
+// weighted-homogeneous points P (degree p, q) and box b, whose block (XY and
+// ZW halves, patch_math.cuh) starts `off` floats into the scene's block
+// array; blk points there.
 NRT_HD inline void pack_slot(const float* P, int p, int q, const Box3& b, int patch_id, int surf, long long off,
                              float* blk, int4& hdr, double4& ctr, float4 corners[4], float& delta,
                              dev::PatchFrame& frame, float4 obb[4]) {
@@ -231,18 +232,18 @@ NRT_HD inline void pack_slot(const float* P, int p, int q, const Box3& b, int pa
         pos = pos && (w > 0.0);
         wmin = fabs(w) < wmin ? fabs(w) : wmin;
         wmax = dmax(wmax, fabs(w));
-        blk[i] = (float)((double)P[4 * i + 0] - w * cx);
-        blk[np + i] = (float)((double)P[4 * i + 1] - w * cy);
-        blk[2 * np + i] = (float)((double)P[4 * i + 2] - w * cz);
-        blk[3 * np + i] = (float)w;
+        blk[dev::block_at(np, i, 0)] = (float)((double)P[4 * i + 0] - w * cx);
+        blk[dev::block_at(np, i, 1)] = (float)((double)P[4 * i + 1] - w * cy);
+        blk[dev::block_at(np, i, 2)] = (float)((double)P[4 * i + 2] - w * cz);
+        blk[dev::block_at(np, i, 3)] = (float)w;
         if (w != 0.0) {
             const double dx = P[4 * i] / w - cx, dy = P[4 * i + 1] / w - cy, dz = P[4 * i + 2] / w - cz;
             rad = dmax(rad, sqrt(dx * dx + dy * dy + dz * dz));
         }
     }
     for (int i = n; i < np; ++i) {  // padding, never read as a point
-        blk[i] = 0.f; blk[np + i] = 0.f; blk[2 * np + i] = 0.f;
-        blk[3 * np + i] = 1.f;
+        blk[dev::block_at(np, i, 0)] = 0.f; blk[dev::block_at(np, i, 1)] = 0.f; blk[dev::block_at(np, i, 2)] = 0.f;
+        blk[dev::block_at(np, i, 3)] = 1.f;
     }
     const int flags = (pos ? dev::kFlagPositiveWeights : 0) | (wmax > dev::kWideWeightRatio * wmin ? dev::kFlagWideWeights : 0);
     hdr = make_int4((int)off, p | (q << 4) | (flags << 8), patch_id, surf);

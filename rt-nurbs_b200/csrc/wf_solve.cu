@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve(Scene sc, WfBuffers wb, int 
             const float u = __uint_as_float((unsigned)(rec.y >> 32)), v = __uint_as_float((unsigned)rec.y);
             const float* __restrict__ blk = sc.cp + h.x;
             float H[4], Hu[4], Hv[4];
-            eval_patch<P, Q, float>(blk, u, v, H, Hu, Hv);
+            eval_patch<P, Q>(blk, u, v, H, Hu, Hv);
             const float iw = __frcp_rn(H[3]);
             const float sx = H[0] * iw, sy = H[1] * iw, sz = H[2] * iw;
             o.fp64_solves = 0;
