@@ -256,13 +256,17 @@ typedef struct {
     int64_t chunk;           /* rays per wavefront pass (bounds the scratch, about 1.1 KB per ray) */
     int32_t quota0;          /* candidates a ray emits in the first round, doubling per round ... */
     int32_t quota_max;       /* ... up to this many (<= 8); the default 4, then 8 */
+    int32_t stage_nodes;     /* nodes of the top of the 4-wide tree (numbered breadth first, so 1, 5, 21,
+                                85 and 341 are whole levels) that each traversal block copies into shared
+                                memory and reads from there; 1 (the default: the root only) to 341 */
 } nrt_wavefront_tuning;
 int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out);
 int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in);
 /* Autotuner: times nrt_intersect (wavefront) on these rays and buffers under
  * candidate launch shapes, one knob at a time (coordinate descent over
- * traversal and scatter grids, class-launch blocks, round quotas and rays
- * per pass; the graph/host-driven choice stays as set), and keeps the
+ * traversal and scatter grids, class-launch blocks, round quotas, the
+ * staged top of the tree and rays per pass; the graph/host-driven choice
+ * stays as set), and keeps the
  * fastest on the scene.  *out gets it and
  * *best_ms its time per call (CUDA events, `reps` calls after one untimed
  * call).  Synchronous.  Results do not depend on the tuning. */

@@ -638,7 +638,8 @@ int nrt_intersect(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
                                           scene->counters, st, &scene->last_launches, &scene->last_rounds,
                                           scene->timing_on ? scene->tev : nullptr,
                                           scene->timing_on ? &scene->newton_ms : nullptr, &scene->newton_launches,
-                                          scene->tuning.quota0, scene->tuning.quota_max);
+                                          scene->tuning.quota0, scene->tuning.quota_max,
+                                          scene->tuning.stage_nodes);
             }
             if (prev != scene->device) cudaSetDevice(prev);
             if (e != cudaSuccess) return cuda_fail(e, "intersect launch");
@@ -687,6 +688,7 @@ int nrt_scene_get_tuning(const nrt_scene* scene, nrt_wavefront_tuning* out) {
     out->chunk = scene->wf_chunk;
     out->quota0 = scene->tuning.quota0;
     out->quota_max = scene->tuning.quota_max;
+    out->stage_nodes = scene->tuning.stage_nodes;
     return NRT_OK;
 }
 
@@ -697,6 +699,8 @@ int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in) {
     if (in->graph > 2) return fail(NRT_ERR_INVALID, "graph must be 1 (graph) or 2 (host-driven)");
     if (in->chunk > (1LL << 30)) return fail(NRT_ERR_INVALID, "chunk above 2^30 rays");
     if (in->quota0 > 8 || in->quota_max > 8) return fail(NRT_ERR_INVALID, "round quotas above 8");
+    if (in->stage_nodes > dev::kMaxStagedNodes)
+        return fail(NRT_ERR_INVALID, "stage_nodes %d above %d", in->stage_nodes, dev::kMaxStagedNodes);
     const int q0 = in->quota0 > 0 ? in->quota0 : scene->tuning.quota0;
     const int qm = in->quota_max > 0 ? in->quota_max : scene->tuning.quota_max;
     if (q0 > qm) return fail(NRT_ERR_INVALID, "quota0 %d above quota_max %d", q0, qm);
@@ -707,6 +711,7 @@ int nrt_scene_set_tuning(nrt_scene* scene, const nrt_wavefront_tuning* in) {
     if (in->chunk > 0) scene->wf_chunk = in->chunk;  // the scratch is re-carved on the next call
     scene->tuning.quota0 = q0;
     scene->tuning.quota_max = qm;
+    if (in->stage_nodes > 0) scene->tuning.stage_nodes = in->stage_nodes;
     return NRT_OK;
 }
 
@@ -751,6 +756,7 @@ int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_in
     const int32_t classes[] = {148 * 2, 148 * 4, 148 * 8, 148 * 16};
     const int64_t chunks[] = {1LL << 21, 1LL << 22, 1LL << 23};
     const int32_t quotas[] = {1 << 8 | 8, 2 << 8 | 8, 4 << 8 | 8, 1 << 8 | 4};  // (first round, cap)
+    const int32_t stages[] = {1, 21, 85, 341};  // whole top levels of the 4-wide tree: none (the root), 3, 4, 5
     for (int pass = 0; pass < 2 && status == NRT_OK; ++pass) {
         auto knob = [&](auto&& values, int count, auto&& set) {
             for (int k = 0; k < count && status == NRT_OK; ++k) {
@@ -784,6 +790,11 @@ int nrt_autotune(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_in
             if (q0 == t.quota0 && qm == t.quota_max) return false;
             t.quota0 = q0;
             t.quota_max = qm;
+            return true;
+        });
+        knob(stages, 4, [&](nrt_wavefront_tuning& t, int32_t v) {
+            if (v == t.stage_nodes) return false;
+            t.stage_nodes = v;
             return true;
         });
         knob(chunks, 3, [&](nrt_wavefront_tuning& t, int64_t v) {
@@ -951,8 +962,9 @@ int noalloc_views(nrt_scene* scene, const nrt_rays* rays, int64_t n, const nrt_i
     v->plan = scene->plan;
     v->counters = scene->counters;
     v->device = scene->device;
-    v->quota0 = scene->tuning.quota0;  // the round quotas nrt_intersect runs with
+    v->quota0 = scene->tuning.quota0;  // the round quotas and staged tree top nrt_intersect runs with
     v->quota_max = scene->tuning.quota_max;
+    v->stage_nodes = scene->tuning.stage_nodes;
     to_dev_opts(o, v->opts, scene->counters_on);
     return NRT_OK;
 }

@@ -91,7 +91,8 @@ extern "C" int nrt_intersect_noalloc(nrt_scene* scene, const nrt_rays* rays, int
         nrt::dev::Opts oc = v.opts;
         oc.seed_offset = v.opts.seed_offset + (uint32_t)at;  // seeds follow the global ray index
         e = nrt::dev::launch_wavefront(v.scene, v.plan, rc, m, oc, hc, wb, &g_round_count[v.device], v.counters, s,
-                                       &launches, &rounds, nullptr, nullptr, nullptr, v.quota0, v.quota_max);
+                                       &launches, &rounds, nullptr, nullptr, nullptr, v.quota0, v.quota_max,
+                                       v.stage_nodes);
     }
     if (prev != v.device) cudaSetDevice(prev);
     if (st != NRT_OK) return st;

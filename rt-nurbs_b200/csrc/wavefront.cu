@@ -71,9 +71,9 @@ struct StepTally {
 // memory and in the saved stacks: one load or store per entry (4.5 % less
 // step time than separate node and distance arrays).  Visiting the nearest
 // child directly, without its push and pop, was slower (register pressure).
-__device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long long n, int round, int j, long long i,
-                                         int quota, const Opts& op, const WfBuffers& wb, int cur, int32_t* tests,
-                                         const int32_t* rank_of, StepTally& c) {
+__device__ __forceinline__ void step_ray(const Scene& sc, const float4* top, int n_top, const Rays& rays, long long n,
+                                         int round, int j, long long i, int quota, const Opts& op, const WfBuffers& wb,
+                                         int cur, int32_t* tests, const int32_t* rank_of, StepTally& c) {
     RayFrame r;
     r.ox = __ldg(rays.ox + i); r.oy = __ldg(rays.oy + i); r.oz = __ldg(rays.oz + i);
     r.dx = __ldg(rays.dx + i); r.dy = __ldg(rays.dy + i); r.dz = __ldg(rays.dz + i);
@@ -99,11 +99,21 @@ __device__ __forceinline__ void step_ray(const Scene& sc, const Rays& rays, long
         const int ref = st[sp].x;
         if (__int_as_float(st[sp].y) >= best) continue;
         if (ref >= 0) {
-            const float4* nd = reinterpret_cast<const float4*>(sc.nodes + ref);
-            const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
-            const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
-            const int4 ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
-            const int4 cn = __ldg(reinterpret_cast<const int4*>(nd + 7));
+            // a node of the staged top of the tree from shared memory, any other through L1
+            float4 lx, hx, ly, hy, lz, hz;
+            int4 ch, cn;
+            if (ref < n_top) {
+                const float4* nd = top + 8 * ref;
+                lx = nd[0]; hx = nd[1]; ly = nd[2]; hy = nd[3]; lz = nd[4]; hz = nd[5];
+                ch = reinterpret_cast<const int4*>(nd)[6];
+                cn = reinterpret_cast<const int4*>(nd)[7];
+            } else {
+                const float4* nd = reinterpret_cast<const float4*>(sc.nodes + ref);
+                lx = __ldg(nd + 0); hx = __ldg(nd + 1); ly = __ldg(nd + 2); hy = __ldg(nd + 3);
+                lz = __ldg(nd + 4); hz = __ldg(nd + 5);
+                ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
+                cn = __ldg(reinterpret_cast<const int4*>(nd + 7));
+            }
             const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
             const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
             const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
@@ -168,14 +178,29 @@ __device__ __forceinline__ void step_count(unsigned long long* ctr, const Opts& 
     if (c.err) atomicAdd(ctr + kErrors, c.err);
 }
 
+// The top of the 4-wide tree in shared memory: the tree is numbered breadth
+// first, so its first `stage` nodes are its top levels (1, 5, 21, 85, 341
+// nodes are whole levels), which every ray entering the tree visits.  The
+// whole block copies them once (eight 16-byte words per node) before any of
+// its threads traverses; returns how many nodes were staged.
+__device__ __forceinline__ int stage_top(const Scene& sc, float4* top, int stage) {
+    const int k = sc.n_nodes < stage ? sc.n_nodes : stage;
+    const float4* src = reinterpret_cast<const float4*>(sc.nodes);
+    for (int w = threadIdx.x; w < 8 * k; w += blockDim.x) top[w] = __ldg(src + w);
+    __syncthreads();
+    return k;
+}
+
 // Host-driven round: the host passes the round, its active count and list.
 __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long n, int round, int n_active,
                                                  int quota, Opts op, WfBuffers wb, int cur, int32_t* tests,
-                                                 unsigned long long* ctr, const int32_t* rank_of) {
+                                                 unsigned long long* ctr, const int32_t* rank_of, int stage) {
+    extern __shared__ float4 top[];
+    const int n_top = stage_top(sc, top, stage);
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     StepTally c{};
     const long long i = j < n_active ? (round == 0 ? (long long)j : (long long)wb.active[cur][j]) : 0;
-    if (j < n_active) step_ray(sc, rays, n, round, j, i, quota, op, wb, cur, tests, rank_of, c);
+    if (j < n_active) step_ray(sc, top, n_top, rays, n, round, j, i, quota, op, wb, cur, tests, rank_of, c);
     step_count(ctr, op, (round == 0 && j < n_active) ? 1ull : 0ull, c);
 }
 
@@ -187,7 +212,9 @@ __global__ void __launch_bounds__(128) k_wf_step(Scene sc, Rays rays, long long 
 // and a round with few active rays costs no empty blocks.
 __global__ void __launch_bounds__(128) k_wf_step_dev(Scene sc, Rays rays, long long n, Opts op, WfBuffers wb,
                                                      int32_t* tests, unsigned long long* ctr, const int32_t* rank_of,
-                                                     int quota0, int quota_max) {
+                                                     int quota0, int quota_max, int stage) {
+    extern __shared__ float4 top[];
+    const int n_top = stage_top(sc, top, stage);  // once per block: the block stays for the whole round
     const int round = wb.counts[2], cur = round & 1;
     const int n_active = round == 0 ? (int)n : wb.counts[cur];
     const int quota = round_quota(round, quota0, quota_max);
@@ -201,7 +228,7 @@ __global__ void __launch_bounds__(128) k_wf_step_dev(Scene sc, Rays rays, long l
         if (base >= n_active) break;
         const int j = base + lane;
         const long long i = j < n_active ? (round == 0 ? (long long)j : (long long)wb.active[cur][j]) : 0;
-        if (j < n_active) step_ray(sc, rays, n, round, j, i, quota, op, wb, cur, tests, rank_of, c);
+        if (j < n_active) step_ray(sc, top, n_top, rays, n, round, j, i, quota, op, wb, cur, tests, rank_of, c);
         if (j < n_active) ++seen;
     }
     step_count(ctr, op, round == 0 ? seen : 0ull, c);
@@ -385,8 +412,10 @@ static void wf_resolve_class(int p, int q, const WfClassLaunch& L) {
 cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& rays, long long n, const Opts& op,
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds, cudaEvent_t* ev,
-                             double* newton_ms, long long* newton_launches, int quota0, int quota_max) {
+                             double* newton_ms, long long* newton_launches, int quota0, int quota_max,
+                             int stage_nodes) {
     if (n <= 0) return cudaSuccess;
+    const int stage = stage_nodes < 1 ? 1 : (stage_nodes > kMaxStagedNodes ? kMaxStagedNodes : stage_nodes);
     cudaError_t e = cudaSuccess;
     int n_active = (int)n, cur = 0;
     WfClassLaunch L{};
@@ -398,9 +427,9 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
         e = cudaMemsetAsync(wb.hist, 0, sizeof(int) * plan.n_slots, stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(wb.counts + (1 - cur), 0, sizeof(int), stream);
         if (e != cudaSuccess) return e;
-        k_wf_step<<<(unsigned)((n_active + 127) / 128), 128, 0, stream>>>(sc, rays, n, round, n_active,
-                                                                         round_quota(round, quota0, quota_max), op, wb,
-                                                                         cur, out.tests, ctr, plan.rank_of);
+        k_wf_step<<<(unsigned)((n_active + 127) / 128), 128, staged_bytes(stage), stream>>>(
+            sc, rays, n, round, n_active, round_quota(round, quota0, quota_max), op, wb, cur, out.tests, ctr,
+            plan.rank_of, stage);
         k_wf_scan<<<1, 1024, 0, stream>>>(plan.n_slots, wb);
         k_wf_scatter<<<(unsigned)((n_active + 255) / 256), 256, 0, stream>>>(rays, round, n_active, wb, cur,
                                                                              plan.rank_of);
@@ -542,8 +571,11 @@ cudaError_t build_wavefront_graph(const Scene& sc, const WfPlan& plan, const Ray
             if (e == cudaSuccess) {
                 const unsigned step_grid = (unsigned)std::max(1LL, std::min<long long>((m + 127) / 128, tu.step_blocks));
                 const unsigned scat_grid = (unsigned)std::max(1LL, std::min<long long>((m + 255) / 256, tu.scatter_blocks));
-                k_wf_step_dev<<<step_grid, 128, 0, cs>>>(sc, rc, m, oc, wb, hc.tests, ctr, plan.rank_of, tu.quota0,
-                                                tu.quota_max);
+                const int stage = tu.stage_nodes < 1 ? 1 : (tu.stage_nodes > kMaxStagedNodes ? kMaxStagedNodes
+                                                                                               : tu.stage_nodes);
+                k_wf_step_dev<<<step_grid, 128, staged_bytes(stage), cs>>>(sc, rc, m, oc, wb, hc.tests, ctr,
+                                                                           plan.rank_of, tu.quota0, tu.quota_max,
+                                                                           stage);
                 k_wf_scan<<<1, 1024, 0, cs>>>(plan.n_slots, wb);
                 k_wf_scatter_dev<<<scat_grid, 256, 0, cs>>>(rc, m, wb, plan.rank_of);
                 fork_classes(cs, side, ev, plan.n_classes, L, [&](int c) {

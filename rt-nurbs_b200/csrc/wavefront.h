@@ -106,7 +106,13 @@ struct WfTuning {
     int class_blocks = 0;               // k_wf_newton blocks of 256 per class launch; 0 = the plan's
     int quota0 = 4;                     // candidates per ray in the first round (doubling each round)
     int quota_max = 8;                  // ... up to this many (<= 8)
+    int stage_nodes = 1;                // top nodes of the tree each traversal block stages in shared memory
 };
+
+// The staged top of the tree: at most the top five levels of the 4-wide tree
+// (341 nodes of 128 bytes, 43.6 KB of shared memory per traversal block).
+constexpr int kMaxStagedNodes = 341;
+inline size_t staged_bytes(int stage) { return (size_t)stage * 128; }
 
 // The whole intersection of n rays as one executable CUDA graph, in passes of
 // `chunk` rays.  Per pass: a set-up kernel, a while-loop node whose body is
@@ -128,7 +134,7 @@ cudaError_t launch_wavefront(const Scene& sc, const WfPlan& plan, const Rays& ra
                              const Hits& out, const WfBuffers& wb, int32_t* host_count, unsigned long long* ctr,
                              cudaStream_t stream, long long* launches, long long* rounds,
                              cudaEvent_t* ev = nullptr, double* newton_ms = nullptr, long long* newton_launches = nullptr,
-                             int quota0 = 1, int quota_max = 8);
+                             int quota0 = 1, int quota_max = 8, int stage_nodes = 1);
 
 // Per-pixel kernel over a device list of ray indices (count read on the device).
 cudaError_t launch_intersect_pixel_list(const Scene& sc, const Rays& rays, const int32_t* list,
@@ -143,7 +149,7 @@ struct NoallocViews {
     dev::Opts opts;
     unsigned long long* counters;
     int device;
-    int quota0, quota_max;
+    int quota0, quota_max, stage_nodes;
 };
 
 }  // namespace nrt

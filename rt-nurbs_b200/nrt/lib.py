@@ -89,7 +89,8 @@ class Counters(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("step_blocks", C.c_int64), ("scatter_blocks", C.c_int64), ("class_blocks", C.c_int32),
-                ("graph", C.c_int32), ("chunk", C.c_int64), ("quota0", C.c_int32), ("quota_max", C.c_int32)]
+                ("graph", C.c_int32), ("chunk", C.c_int64), ("quota0", C.c_int32), ("quota_max", C.c_int32),
+                ("stage_nodes", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -132,8 +132,9 @@ def test_clip_cull_changes_nothing(nrt_gpu):
 
 
 def test_tuning_changes_nothing_and_autotune(nrt_gpu):
-    """Launch shapes (graph or host-driven rounds, grid sizes, rays per pass)
-    change no result bit; the autotuner picks one of them."""
+    """Launch shapes (graph or host-driven rounds, grid sizes, rays per pass,
+    the staged top of the tree) change no result bit; the autotuner picks one
+    of them."""
     from nrt import scenes
 
     sc = scenes.surfaces_grid_scene(16, seed=5, width=320, height=180, spp=2)
@@ -144,8 +145,11 @@ def test_tuning_changes_nothing_and_autotune(nrt_gpu):
     base = to_numpy(scene.intersect(rays, opts))
     c0 = scene.counters()
     assert c0["rounds"] > 1 and c0["kernel_launches"] > c0["rounds"]
+    # (set_tuning keeps the fields a variant leaves out: the staged-top variants come before the quota
+    # variants, so that they run with the default quotas and their per-ray test counts can be compared)
     for kw in [dict(graph=2), dict(graph=1, step_blocks=37, scatter_blocks=11, class_blocks=5),
-               dict(graph=1, chunk=10007), dict(graph=2, chunk=4096), dict(graph=1, quota0=8, quota_max=8),
+               dict(graph=1, chunk=10007), dict(graph=2, chunk=4096), dict(graph=1, stage_nodes=341),
+               dict(graph=2, stage_nodes=85), dict(graph=1, stage_nodes=1), dict(graph=1, quota0=8, quota_max=8),
                dict(graph=2, quota0=1, quota_max=1), dict(graph=1, quota0=2, quota_max=4)]:
         scene.set_tuning(**kw)
         b = to_numpy(scene.intersect(rays, opts))
