@@ -110,8 +110,8 @@ int nrt_build_bvh_binary(const float* boxes, int n, int builder, float* node_bou
 /* ------------------------------------------------------------------------
  * Scenes: decomposition + BVH + device upload in one call (the host pipeline
  * of src/core/main.cpp:104-149 / src/core/benchmark.cpp:163-186).  The scene
- * keeps its own device copy (patches packed SoA per patch, 16-byte aligned,
- * in patch-local coordinates; a 4-wide BVH).  Patch ids reported by
+ * keeps its own device copy (each patch's points as (x, y) and (z, w) pair
+ * arrays, 16-byte aligned, in patch-local coordinates; a 4-wide BVH).  Patch ids reported by
  * nrt_intersect are global patch indices in creation order: surface 0's
  * patches first, each surface in getPatch order. */
 typedef struct nrt_scene nrt_scene;
