@@ -264,3 +264,40 @@ def test_binned_bvh_matches_restatement(nrt_mod, oracle_mod, n_surfaces, seed):
     assert orc.used == used and np.array_equal(orc.order, ref[3])
     assert np.array_equal(orc.lf[:used], ref[1][:used]) and np.array_equal(orc.cnt[:used], ref[2][:used])
     assert np.array_equal(orc.box[:used], ref[0][:used])
+
+
+def test_ctypes_mirrors_match_header(tmp_path):
+    """Every struct of include/nrt.h that the ctypes binding (nrt/lib.py)
+    mirrors has the same size and the same field offsets: a C program built on
+    the header with the system compiler prints sizeof and offsetof for each
+    mirrored field.  A field added on one side only would make the library
+    read or write past the caller's struct."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from nrt import lib_module as L
+
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    mirrors = {"nrt_nurbs_surface": L.NurbsSurface, "nrt_build_opts": L.BuildOpts, "nrt_scene_info": L.SceneInfo,
+               "nrt_rays": L.RaysC, "nrt_hits": L.HitsC, "nrt_intersect_opts": L.IntersectOpts,
+               "nrt_wavefront_tuning": L.Tuning, "nrt_counters": L.Counters, "nrt_train_opts": L.TrainOpts,
+               "nrt_camera": L.CameraC}
+    src = ["#include <stdio.h>", "#include <stddef.h>", '#include "nrt.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        src.append(f'printf("{cname} . %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            src.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    src += ["return 0;", "}"]
+    c_file, exe = tmp_path / "layout.c", tmp_path / "layout"
+    c_file.write_text("\n".join(src) + "\n")
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(c_file)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, field, value = line.split()
+        got[(cname, field)] = int(value)
+    for cname, cls in mirrors.items():
+        assert got[(cname, ".")] == ctypes.sizeof(cls), (cname, got[(cname, ".")], ctypes.sizeof(cls))
+        for f, _ in cls._fields_:
+            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)
